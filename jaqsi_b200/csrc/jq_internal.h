@@ -1,0 +1,147 @@
+// Internal data model shared by the host planner (planner.cpp) and the device
+// kernels (kernels.cu).  Nothing here crosses the C ABI.
+#pragma once
+
+#include <array>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/jqsim.h"
+
+namespace jq {
+
+constexpr int kMaxBlockWires = 6;   // widest fused block on the (2n-)bit vector
+constexpr int kMaxTileBits = 15;    // tile = 2^t amplitudes held by one CTA
+constexpr int kMaxFusePrims = 16;   // longest same-wire fusion run
+
+// How a block is applied inside a tile.
+enum BlockKind : int32_t { BK_DENSE = 0, BK_DIAG = 1, BK_PERM = 2 };
+
+// How a prim's full matrix is obtained from its op.
+enum PrimForm : int32_t {
+  PF_U = 0,     // the op's matrix U
+  PF_CONJ = 1,  // conj(U)           (bra side of a wide gate on a density matrix)
+  PF_KRON = 2,  // kron(U, conj(U))  (superoperator of a 1-qubit gate)
+  PF_CONST = 3  // constant matrix from the plan's constant pool
+};
+
+// Static guarantees of a matrix (jaqsi GateStructure, operations.py:176-185).
+struct Structure {
+  std::vector<int32_t> perm;  // empty: no permutation guarantee
+  bool diagonal = false;
+  int32_t controls = 0;
+};
+
+// Device descriptor of a recorded op (matrix construction).
+struct DevOp {
+  int32_t kind;        // jq_op_kind
+  int32_t k;           // op wires
+  int32_t n_ctrl;      // PAULIROT controls
+  int32_t angle_slot;
+  int32_t mat_slot;
+  int32_t mat_is_diag;
+  uint32_t px, pz;     // PAULIROT word masks over target positions
+  int32_t grad;
+  int32_t n_angles;    // parameters of the op
+};
+
+// Device descriptor of a prim (one factor of a fused block).
+struct DevPrim {
+  int32_t op;          // DevOp index, -1 for constants without an op
+  int32_t form;        // PrimForm
+  int32_t k;           // wires of the prim on the bit vector
+  int32_t const_off;   // PF_CONST: complex128 offset in the constant pool
+};
+
+// Device descriptor of a fused block.
+struct DevBlock {
+  int32_t kind;        // BlockKind
+  int32_t k;           // wires
+  int32_t n_ctrl;      // leading control wires
+  int32_t d;           // inner dimension 2^(k - n_ctrl)
+  int32_t prim_begin, prim_end;
+  int32_t mat_off;     // run-dtype complex offset of the inner matrix / diagonal
+  int32_t perm_off;    // BK_PERM: offset of the inner permutation in the perm pool
+  int32_t grad_off;    // complex128 offset of the cotangent accumulator, -1 if none
+  int32_t scratch_off; // complex128 offset of per-instance scratch (k > 2), -1 if none
+};
+
+// One block application inside a tile pass (tile-local bit positions).
+struct TileOp {
+  int32_t block;
+  int32_t kind;
+  int32_t kt;          // target bits
+  int32_t nfix;        // target + control bits
+  uint32_t ctrl_mask;  // tile-local mask of the control bits (all must be 1)
+  int8_t fix[kMaxBlockWires];  // fixed bits, ascending
+  int8_t tb[kMaxBlockWires];   // target bits, tb[0] = most significant matrix bit
+  int32_t mat_off, perm_off, grad_off;
+};
+
+// One HBM pass: a tile covers the bits of `tile_mask`.
+struct PassDesc {
+  int32_t t;           // tile bits
+  int32_t c;           // tile bits 0..c-1 are global bits 0..c-1
+  uint64_t tile_mask;  // global bits held in the tile
+  int32_t op_begin, op_end;
+  int8_t bits[kMaxTileBits];  // global bit of each tile bit, ascending
+};
+
+struct Schedule {
+  int32_t t = 0;
+  std::vector<PassDesc> passes;
+  std::vector<TileOp> ops;
+};
+
+// Device copies of a plan's tables on one GPU.
+struct DeviceTables {
+  int device = -1;
+  DevOp* ops = nullptr;
+  DevPrim* prims = nullptr;
+  DevBlock* blocks = nullptr;
+  TileOp* fwd_ops = nullptr;
+  TileOp* adj_ops = nullptr;
+  TileOp* bwd_ops = nullptr;
+  double* const_pool = nullptr;   // complex128 (re, im) pairs
+  int32_t* perm_pool = nullptr;
+  double* obs_pool = nullptr;     // dense observables, complex128
+  void* obs_desc = nullptr;       // DevObs array
+};
+
+struct DevObs {
+  int32_t kind;        // jq_obs_kind
+  int32_t k;
+  uint64_t x_mask, z_mask;  // PAULI, flat-index bits
+  int32_t n_y;
+  double coeff;
+  int32_t mat_off;     // DENSE: complex128 offset in obs_pool
+  int8_t bits[JQ_MAX_OP_WIRES];  // DENSE: flat-index bit of each wire (wire 0 = MSB of matrix)
+};
+
+}  // namespace jq
+
+struct jq_plan {
+  int n_qubits = 0;
+  int n_bits = 0;
+  int mode = 0, dtype = 0;
+  int n_angles = 0, n_mats = 0;
+  bool unitary = true;
+  bool any_grad = false;
+  int64_t state_elems = 0;
+  std::vector<jq::DevOp> ops;
+  std::vector<jq::DevPrim> prims;
+  std::vector<jq::DevBlock> blocks;
+  std::vector<std::array<int32_t, jq::kMaxBlockWires>> block_wires;  // wires per block, -1 padded
+  std::vector<double> const_pool;
+  std::vector<int32_t> perm_pool;
+  std::vector<jq::DevObs> obs;
+  std::vector<double> obs_pool;
+  jq::Schedule fwd, adj, bwd;  // bwd: one block per pass (checkpointed reverse)
+  int64_t bmat_stride = 0;     // run-dtype complex elements per instance
+  int64_t grad_stride = 0;     // complex128 elements per instance
+  int64_t scratch_stride = 0;  // complex128 elements per instance (k > 2 blocks)
+  int threads = 512;
+  int ckpt_stride = 0;
+  std::vector<jq::DeviceTables> dev;  // per-device uploads
+};

@@ -1,0 +1,1780 @@
+// libjqsim: sm_100a kernels and the C ABI of the circuit-execution backend.
+//
+// The state (a 2^n statevector or a 4^n density matrix seen as a 2n-bit
+// vector) lives in caller-owned HBM.  A forward sweep is a short list of tile
+// passes: each CTA stages a tile of 2^t amplitudes (t qubits, always including
+// the low qubits for coalescing) in shared memory, applies every fused gate
+// block of the pass that acts inside the tile, and writes the tile back.  One
+// pass therefore replaces the reference's one-XLA-loop-per-entry
+// (jaqsi/simulation.py:400-409) for all the blocks it holds.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+
+#include "jq_internal.h"
+#include "kernels.cuh"
+
+namespace jq {
+void set_error(const std::string& msg);
+extern thread_local std::string g_last_error;
+int build_plan(const jq_op* ops, int n_ops, const jq_obs* obs, int n_obs, int n_qubits, int mode, int dtype,
+               const jq_tune* tune, jq_plan** out);
+}  // namespace jq
+
+namespace jq {
+namespace {
+
+constexpr int kRedSlots = 64;  // doubles per warp in the block-reduction scratch
+
+// ---------------------------------------------------------------------------
+// index helpers
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint64_t pdep64(uint64_t v, uint64_t mask) {
+  uint64_t r = 0;
+  for (uint64_t bb = 1; mask; bb <<= 1) {
+    uint64_t low = mask & (~mask + 1);
+    if (v & bb) r |= low;
+    mask &= mask - 1;
+  }
+  return r;
+}
+
+__device__ __forceinline__ int group_base(int g, const TileOp& op) {
+  int b = g;
+  for (int i = 0; i < op.nfix; ++i) {
+    const int p = op.fix[i];
+    b = ((b >> p) << (p + 1)) | (b & ((1 << p) - 1));
+  }
+  return b | static_cast<int>(op.ctrl_mask);
+}
+
+__device__ __forceinline__ int target_off(int j, const TileOp& op, int kt) {
+  int o = 0;
+  for (int i = 0; i < kt; ++i)
+    if ((j >> (kt - 1 - i)) & 1) o |= 1 << op.tb[i];
+  return o;
+}
+
+// Sum `nv` per-thread doubles over the CTA; thread v < nv receives total v.
+__device__ inline void block_reduce(double* vals, int nv, double* red) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int v = 0; v < nv; ++v) {
+    double x = vals[v];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    vals[v] = x;
+  }
+  __syncthreads();
+  if (lane == 0)
+    for (int v = 0; v < nv; ++v) red[warp * kRedSlots + v] = vals[v];
+  __syncthreads();
+  if (threadIdx.x < nv) {
+    double s = 0.0;
+    for (int w = 0; w < nw; ++w) s += red[w * kRedSlots + threadIdx.x];
+    vals[0] = s;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// block application inside a tile (forward: G, adjoint: G^dagger)
+// ---------------------------------------------------------------------------
+template <typename C, int KT>
+__device__ void tile_dense(C* s, int t, const TileOp& op, const C* __restrict__ M, bool dag) {
+  constexpr int D = 1 << KT;
+  const int G = 1 << (t - op.nfix);
+  int off[D];
+#pragma unroll
+  for (int j = 0; j < D; ++j) off[j] = target_off(j, op, KT);
+  C m[D * D];
+#pragma unroll
+  for (int i = 0; i < D; ++i)
+#pragma unroll
+    for (int j = 0; j < D; ++j) m[i * D + j] = dag ? cconj(M[j * D + i]) : M[i * D + j];
+  for (int g = threadIdx.x; g < G; g += blockDim.x) {
+    const int base = group_base(g, op);
+    C v[D];
+#pragma unroll
+    for (int j = 0; j < D; ++j) v[j] = s[base + off[j]];
+#pragma unroll
+    for (int i = 0; i < D; ++i) {
+      C acc = cmake<C>(0, 0);
+#pragma unroll
+      for (int j = 0; j < D; ++j) acc = cfma(m[i * D + j], v[j], acc);
+      s[base + off[i]] = acc;
+    }
+  }
+}
+
+// Blocks on 3..6 target bits (rare): dynamic loops, group held in local memory.
+template <typename C>
+__device__ void tile_dense_wide(C* s, int t, const TileOp& op, const C* __restrict__ M, bool dag) {
+  const int kt = op.kt, D = 1 << kt;
+  const int G = 1 << (t - op.nfix);
+  for (int g = threadIdx.x; g < G; g += blockDim.x) {
+    const int base = group_base(g, op);
+    C v[64];
+#pragma unroll 1
+    for (int j = 0; j < D; ++j) v[j] = s[base + target_off(j, op, kt)];
+#pragma unroll 1
+    for (int i = 0; i < D; ++i) {
+      C acc = cmake<C>(0, 0);
+#pragma unroll 1
+      for (int j = 0; j < D; ++j) acc = cfma(dag ? cconj(M[j * D + i]) : M[i * D + j], v[j], acc);
+      s[base + target_off(i, op, kt)] = acc;
+    }
+  }
+}
+
+template <typename C>
+__device__ void tile_diag(C* s, int t, const TileOp& op, const C* __restrict__ Dg, bool dag) {
+  const int kt = op.kt, D = 1 << kt;
+  const int G = 1 << (t - op.nfix);
+  const int total = G * D;
+  for (int e = threadIdx.x; e < total; e += blockDim.x) {
+    const int g = e >> kt, j = e & (D - 1);
+    const int idx = group_base(g, op) + target_off(j, op, kt);
+    const C d = dag ? cconj(Dg[j]) : Dg[j];
+    s[idx] = cmul(d, s[idx]);
+  }
+}
+
+template <typename C, int KT>
+__device__ void tile_perm(C* s, int t, const TileOp& op, const int* __restrict__ P, bool inv) {
+  constexpr int D = 1 << KT;
+  const int G = 1 << (t - op.nfix);
+  int off[D], p[D];
+#pragma unroll
+  for (int j = 0; j < D; ++j) {
+    off[j] = target_off(j, op, KT);
+    p[j] = P[j];
+  }
+  for (int g = threadIdx.x; g < G; g += blockDim.x) {
+    const int base = group_base(g, op);
+    C v[D];
+#pragma unroll
+    for (int j = 0; j < D; ++j) v[j] = s[base + off[j]];
+    if (!inv) {
+#pragma unroll
+      for (int i = 0; i < D; ++i) s[base + off[i]] = v[p[i]];
+    } else {
+#pragma unroll
+      for (int i = 0; i < D; ++i) s[base + off[p[i]]] = v[i];
+    }
+  }
+}
+
+template <typename C>
+__device__ void tile_perm_wide(C* s, int t, const TileOp& op, const int* __restrict__ P, bool inv) {
+  const int kt = op.kt, D = 1 << kt;
+  const int G = 1 << (t - op.nfix);
+  for (int g = threadIdx.x; g < G; g += blockDim.x) {
+    const int base = group_base(g, op);
+    C v[64];
+#pragma unroll 1
+    for (int j = 0; j < D; ++j) v[j] = s[base + target_off(j, op, kt)];
+#pragma unroll 1
+    for (int i = 0; i < D; ++i) {
+      if (!inv) s[base + target_off(i, op, kt)] = v[P[i]];
+      else s[base + target_off(P[i], op, kt)] = v[i];
+    }
+  }
+}
+
+template <typename C>
+__device__ void tile_apply(C* s, int t, const TileOp& op, const C* bm, const int* perms, bool dag) {
+  switch (op.kind) {
+    case BK_DENSE:
+      switch (op.kt) {
+        case 1: tile_dense<C, 1>(s, t, op, bm + op.mat_off, dag); break;
+        case 2: tile_dense<C, 2>(s, t, op, bm + op.mat_off, dag); break;
+        default: tile_dense_wide<C>(s, t, op, bm + op.mat_off, dag); break;
+      }
+      break;
+    case BK_DIAG: tile_diag<C>(s, t, op, bm + op.mat_off, dag); break;
+    default:
+      switch (op.kt) {
+        case 1: tile_perm<C, 1>(s, t, op, perms + op.perm_off, dag); break;
+        case 2: tile_perm<C, 2>(s, t, op, perms + op.perm_off, dag); break;
+        default: tile_perm_wide<C>(s, t, op, perms + op.perm_off, dag); break;
+      }
+      break;
+  }
+}
+
+// Tile geometry shared by the pass kernels.
+struct TileGeo {
+  int t, c;
+  int64_t tiles_per;
+  uint64_t outer_mask;
+};
+
+__device__ __forceinline__ void fill_table(uint32_t* tbl, const PassDesc& pd) {
+  const int nhi = pd.t - pd.c;
+  for (int h = threadIdx.x; h < (1 << nhi); h += blockDim.x) {
+    uint32_t o = 0;
+    for (int i = 0; i < nhi; ++i)
+      if ((h >> i) & 1) o |= 1u << pd.bits[pd.c + i];
+    tbl[h] = o;
+  }
+}
+
+template <typename C>
+__device__ __forceinline__ void tile_load(C* s, const C* g, const uint32_t* tbl, int t, int c) {
+  const int cm = (1 << c) - 1;
+  for (int l = threadIdx.x; l < (1 << t); l += blockDim.x) s[l] = g[tbl[l >> c] | (l & cm)];
+}
+template <typename C>
+__device__ __forceinline__ void tile_store(const C* s, C* g, const uint32_t* tbl, int t, int c) {
+  const int cm = (1 << c) - 1;
+  for (int l = threadIdx.x; l < (1 << t); l += blockDim.x) g[tbl[l >> c] | (l & cm)] = s[l];
+}
+
+// ---------------------------------------------------------------------------
+// forward tile pass
+// ---------------------------------------------------------------------------
+template <typename R>
+__global__ void __launch_bounds__(1024) k_tile_fwd(typename CplxT<R>::T* __restrict__ state, int nb, int batch,
+                                                   PassDesc pd, const TileOp* __restrict__ ops,
+                                                   const typename CplxT<R>::T* __restrict__ bmat, int64_t bmat_stride,
+                                                   const int* __restrict__ perms) {
+  using C = typename CplxT<R>::T;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* s = reinterpret_cast<C*>(smem_raw);
+  const int t = pd.t, c = pd.c;
+  uint32_t* tbl = reinterpret_cast<uint32_t*>(s + (1 << t));
+  fill_table(tbl, pd);
+  const int64_t tiles_per = 1LL << (nb - t);
+  const int64_t ntiles = tiles_per * batch;
+  const uint64_t full = (nb >= 64) ? ~0ULL : ((1ULL << nb) - 1);
+  const uint64_t outer_mask = full & ~pd.tile_mask;
+  for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int64_t inst = tile >> (nb - t);
+    const uint64_t ti = static_cast<uint64_t>(tile) & static_cast<uint64_t>(tiles_per - 1);
+    C* g = state + (inst << nb) + pdep64(ti, outer_mask);
+    const C* bm = bmat + inst * bmat_stride;
+    __syncthreads();
+    tile_load(s, g, tbl, t, c);
+    __syncthreads();
+    for (int oi = pd.op_begin; oi < pd.op_end; ++oi) {
+      const TileOp op = ops[oi];
+      tile_apply<C>(s, t, op, bm, perms, false);
+      __syncthreads();
+    }
+    tile_store(s, g, tbl, t, c);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// adjoint tile pass: psi <- G^dagger psi, grad += lam psi^dagger, lam <- G^dagger lam
+// ---------------------------------------------------------------------------
+template <typename C, int KT>
+__device__ void adj_dense(C* sp, C* sl, int t, const TileOp& op, const C* __restrict__ M, double2* gacc,
+                          double* red) {
+  constexpr int D = 1 << KT;
+  const int G = 1 << (t - op.nfix);
+  const bool grad = op.grad_off >= 0;
+  int off[D];
+#pragma unroll
+  for (int j = 0; j < D; ++j) off[j] = target_off(j, op, KT);
+  C mh[D * D];  // M^dagger
+#pragma unroll
+  for (int i = 0; i < D; ++i)
+#pragma unroll
+    for (int j = 0; j < D; ++j) mh[i * D + j] = cconj(M[j * D + i]);
+  double2 acc[D * D];
+#pragma unroll
+  for (int e = 0; e < D * D; ++e) acc[e] = make_double2(0, 0);
+  for (int g = threadIdx.x; g < G; g += blockDim.x) {
+    const int base = group_base(g, op);
+    C vp[D], vl[D], np[D];
+#pragma unroll
+    for (int j = 0; j < D; ++j) {
+      vp[j] = sp[base + off[j]];
+      vl[j] = sl[base + off[j]];
+    }
+    // psi_{k-1} = G^dagger psi_k
+#pragma unroll
+    for (int i = 0; i < D; ++i) {
+      C a = cmake<C>(0, 0);
+#pragma unroll
+      for (int j = 0; j < D; ++j) a = cfma(mh[i * D + j], vp[j], a);
+      np[i] = a;
+      sp[base + off[i]] = a;
+    }
+    if (grad) {
+#pragma unroll
+      for (int i = 0; i < D; ++i) {
+        const double2 li = to_d2(vl[i]);
+#pragma unroll
+        for (int j = 0; j < D; ++j) acc[i * D + j] = cfma(li, cconj(to_d2(np[j])), acc[i * D + j]);
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < D; ++i) {
+      C a = cmake<C>(0, 0);
+#pragma unroll
+      for (int j = 0; j < D; ++j) a = cfma(mh[i * D + j], vl[j], a);
+      sl[base + off[i]] = a;
+    }
+  }
+  if (grad) {
+    double vals[2 * D * D];
+#pragma unroll
+    for (int e = 0; e < D * D; ++e) {
+      vals[2 * e] = acc[e].x;
+      vals[2 * e + 1] = acc[e].y;
+    }
+    block_reduce(vals, 2 * D * D, red);
+    if (threadIdx.x < 2 * D * D) atomicAdd(reinterpret_cast<double*>(gacc + op.grad_off) + threadIdx.x, vals[0]);
+  }
+}
+
+// Wide blocks (3..6 target bits): dynamic loops, gradient by direct atomics.
+template <typename C>
+__device__ void adj_dense_wide(C* sp, C* sl, int t, const TileOp& op, const C* __restrict__ M, double2* gacc) {
+  const int kt = op.kt, D = 1 << kt;
+  const int G = 1 << (t - op.nfix);
+  const bool grad = op.grad_off >= 0;
+  for (int g = threadIdx.x; g < G; g += blockDim.x) {
+    const int base = group_base(g, op);
+    C vp[64], vl[64], np[64];
+#pragma unroll 1
+    for (int j = 0; j < D; ++j) {
+      vp[j] = sp[base + target_off(j, op, kt)];
+      vl[j] = sl[base + target_off(j, op, kt)];
+    }
+#pragma unroll 1
+    for (int i = 0; i < D; ++i) {
+      C a = cmake<C>(0, 0), b = cmake<C>(0, 0);
+#pragma unroll 1
+      for (int j = 0; j < D; ++j) {
+        const C mh = cconj(M[j * D + i]);
+        a = cfma(mh, vp[j], a);
+        b = cfma(mh, vl[j], b);
+      }
+      np[i] = a;
+      sp[base + target_off(i, op, kt)] = a;
+      sl[base + target_off(i, op, kt)] = b;
+    }
+    if (grad) {
+#pragma unroll 1
+      for (int i = 0; i < D; ++i)
+#pragma unroll 1
+        for (int j = 0; j < D; ++j) {
+          const double2 v = cmul(to_d2(vl[i]), cconj(to_d2(np[j])));
+          atomicAdd(&gacc[op.grad_off + i * D + j].x, v.x);
+          atomicAdd(&gacc[op.grad_off + i * D + j].y, v.y);
+        }
+    }
+  }
+}
+
+template <typename C>
+__device__ void adj_diag(C* sp, C* sl, int t, const TileOp& op, const C* __restrict__ Dg, double2* gacc,
+                         double* red) {
+  const int kt = op.kt, D = 1 << kt;
+  const int G = 1 << (t - op.nfix);
+  const bool grad = op.grad_off >= 0;
+  const int total = G * D;
+  double2 acc[4];
+  for (int e = 0; e < 4; ++e) acc[e] = make_double2(0, 0);
+  for (int e = threadIdx.x; e < total; e += blockDim.x) {
+    const int g = e >> kt, j = e & (D - 1);
+    const int idx = group_base(g, op) + target_off(j, op, kt);
+    const C dc = cconj(Dg[j]);
+    const C np = cmul(dc, sp[idx]);
+    const C l = sl[idx];
+    sp[idx] = np;
+    sl[idx] = cmul(dc, l);
+    if (grad) {
+      const double2 v = cmul(to_d2(l), cconj(to_d2(np)));
+      if (kt <= 2) {
+        // j < 4: keep in registers
+        for (int q = 0; q < 4; ++q)
+          if (q == j) acc[q] = cadd(acc[q], v);
+      } else {
+        atomicAdd(&gacc[op.grad_off + j].x, v.x);
+        atomicAdd(&gacc[op.grad_off + j].y, v.y);
+      }
+    }
+  }
+  if (grad && kt <= 2) {
+    double vals[8];
+    for (int q = 0; q < 4; ++q) {
+      vals[2 * q] = acc[q].x;
+      vals[2 * q + 1] = acc[q].y;
+    }
+    block_reduce(vals, 2 * D, red);
+    if (threadIdx.x < 2 * D) atomicAdd(reinterpret_cast<double*>(gacc + op.grad_off) + threadIdx.x, vals[0]);
+  }
+}
+
+template <typename C>
+__device__ void adj_apply(C* sp, C* sl, int t, const TileOp& op, const C* bm, const int* perms, double2* gacc,
+                          double* red) {
+  switch (op.kind) {
+    case BK_DENSE:
+      switch (op.kt) {
+        case 1: adj_dense<C, 1>(sp, sl, t, op, bm + op.mat_off, gacc, red); break;
+        case 2: adj_dense<C, 2>(sp, sl, t, op, bm + op.mat_off, gacc, red); break;
+        default: adj_dense_wide<C>(sp, sl, t, op, bm + op.mat_off, gacc); break;
+      }
+      break;
+    case BK_DIAG: adj_diag<C>(sp, sl, t, op, bm + op.mat_off, gacc, red); break;
+    default:
+      tile_apply<C>(sp, t, op, bm, perms, true);
+      tile_apply<C>(sl, t, op, bm, perms, true);
+      break;
+  }
+}
+
+template <typename R>
+__global__ void __launch_bounds__(1024) k_tile_adj(typename CplxT<R>::T* __restrict__ psi,
+                                                   typename CplxT<R>::T* __restrict__ lam, int nb, int batch,
+                                                   PassDesc pd, const TileOp* __restrict__ ops,
+                                                   const typename CplxT<R>::T* __restrict__ bmat, int64_t bmat_stride,
+                                                   const int* __restrict__ perms, double2* gacc, int64_t grad_stride) {
+  using C = typename CplxT<R>::T;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int t = pd.t, c = pd.c;
+  C* sp = reinterpret_cast<C*>(smem_raw);
+  C* sl = sp + (1 << t);
+  double* red = reinterpret_cast<double*>(sl + (1 << t));
+  uint32_t* tbl = reinterpret_cast<uint32_t*>(red + 32 * kRedSlots);
+  fill_table(tbl, pd);
+  const int64_t tiles_per = 1LL << (nb - t);
+  const int64_t ntiles = tiles_per * batch;
+  const uint64_t full = (nb >= 64) ? ~0ULL : ((1ULL << nb) - 1);
+  const uint64_t outer_mask = full & ~pd.tile_mask;
+  for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int64_t inst = tile >> (nb - t);
+    const uint64_t ti = static_cast<uint64_t>(tile) & static_cast<uint64_t>(tiles_per - 1);
+    const uint64_t o = (inst << nb) + pdep64(ti, outer_mask);
+    const C* bm = bmat + inst * bmat_stride;
+    double2* ga = gacc ? gacc + inst * grad_stride : nullptr;
+    __syncthreads();
+    tile_load(sp, psi + o, tbl, t, c);
+    tile_load(sl, lam + o, tbl, t, c);
+    __syncthreads();
+    for (int oi = pd.op_end - 1; oi >= pd.op_begin; --oi) {
+      TileOp op = ops[oi];
+      if (!ga) op.grad_off = -1;
+      adj_apply<C>(sp, sl, t, op, bm, perms, ga, red);
+      __syncthreads();
+    }
+    tile_store(sp, psi + o, tbl, t, c);
+    tile_store(sl, lam + o, tbl, t, c);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// checkpointed reverse step: one block, x is the block's input (kept), lam is
+// pulled back through G (lam <- G^dagger lam) and grad += lam x^dagger.
+// ---------------------------------------------------------------------------
+template <typename C, int KT>
+__device__ void bwd_dense(const C* sx, C* sl, int t, const TileOp& op, const C* __restrict__ M, double2* gacc,
+                          double* red) {
+  constexpr int D = 1 << KT;
+  const int G = 1 << (t - op.nfix);
+  const bool grad = op.grad_off >= 0;
+  int off[D];
+#pragma unroll
+  for (int j = 0; j < D; ++j) off[j] = target_off(j, op, KT);
+  C mh[D * D];
+#pragma unroll
+  for (int i = 0; i < D; ++i)
+#pragma unroll
+    for (int j = 0; j < D; ++j) mh[i * D + j] = cconj(M[j * D + i]);
+  double2 acc[D * D];
+#pragma unroll
+  for (int e = 0; e < D * D; ++e) acc[e] = make_double2(0, 0);
+  for (int g = threadIdx.x; g < G; g += blockDim.x) {
+    const int base = group_base(g, op);
+    C vx[D], vl[D];
+#pragma unroll
+    for (int j = 0; j < D; ++j) {
+      vx[j] = sx[base + off[j]];
+      vl[j] = sl[base + off[j]];
+    }
+    if (grad) {
+#pragma unroll
+      for (int i = 0; i < D; ++i)
+#pragma unroll
+        for (int j = 0; j < D; ++j) acc[i * D + j] = cfma(to_d2(vl[i]), cconj(to_d2(vx[j])), acc[i * D + j]);
+    }
+#pragma unroll
+    for (int i = 0; i < D; ++i) {
+      C a = cmake<C>(0, 0);
+#pragma unroll
+      for (int j = 0; j < D; ++j) a = cfma(mh[i * D + j], vl[j], a);
+      sl[base + off[i]] = a;
+    }
+  }
+  if (grad) {
+    double vals[2 * D * D];
+#pragma unroll
+    for (int e = 0; e < D * D; ++e) {
+      vals[2 * e] = acc[e].x;
+      vals[2 * e + 1] = acc[e].y;
+    }
+    block_reduce(vals, 2 * D * D, red);
+    if (threadIdx.x < 2 * D * D) atomicAdd(reinterpret_cast<double*>(gacc + op.grad_off) + threadIdx.x, vals[0]);
+  }
+}
+
+template <typename C>
+__device__ void bwd_dense_wide(const C* sx, C* sl, int t, const TileOp& op, const C* __restrict__ M,
+                               double2* gacc) {
+  const int kt = op.kt, D = 1 << kt;
+  const int G = 1 << (t - op.nfix);
+  const bool grad = op.grad_off >= 0;
+  for (int g = threadIdx.x; g < G; g += blockDim.x) {
+    const int base = group_base(g, op);
+    C vx[64], vl[64];
+#pragma unroll 1
+    for (int j = 0; j < D; ++j) {
+      vx[j] = sx[base + target_off(j, op, kt)];
+      vl[j] = sl[base + target_off(j, op, kt)];
+    }
+    if (grad) {
+#pragma unroll 1
+      for (int i = 0; i < D; ++i)
+#pragma unroll 1
+        for (int j = 0; j < D; ++j) {
+          const double2 v = cmul(to_d2(vl[i]), cconj(to_d2(vx[j])));
+          atomicAdd(&gacc[op.grad_off + i * D + j].x, v.x);
+          atomicAdd(&gacc[op.grad_off + i * D + j].y, v.y);
+        }
+    }
+#pragma unroll 1
+    for (int i = 0; i < D; ++i) {
+      C a = cmake<C>(0, 0);
+#pragma unroll 1
+      for (int j = 0; j < D; ++j) a = cfma(cconj(M[j * D + i]), vl[j], a);
+      sl[base + target_off(i, op, kt)] = a;
+    }
+  }
+}
+
+template <typename C>
+__device__ void bwd_diag(const C* sx, C* sl, int t, const TileOp& op, const C* __restrict__ Dg, double2* gacc,
+                         double* red) {
+  const int kt = op.kt, D = 1 << kt;
+  const int G = 1 << (t - op.nfix);
+  const bool grad = op.grad_off >= 0;
+  const int total = G * D;
+  double2 acc[4];
+  for (int e = 0; e < 4; ++e) acc[e] = make_double2(0, 0);
+  for (int e = threadIdx.x; e < total; e += blockDim.x) {
+    const int g = e >> kt, j = e & (D - 1);
+    const int idx = group_base(g, op) + target_off(j, op, kt);
+    const C l = sl[idx];
+    sl[idx] = cmul(cconj(Dg[j]), l);
+    if (grad) {
+      const double2 v = cmul(to_d2(l), cconj(to_d2(sx[idx])));
+      if (kt <= 2) {
+        for (int q = 0; q < 4; ++q)
+          if (q == j) acc[q] = cadd(acc[q], v);
+      } else {
+        atomicAdd(&gacc[op.grad_off + j].x, v.x);
+        atomicAdd(&gacc[op.grad_off + j].y, v.y);
+      }
+    }
+  }
+  if (grad && kt <= 2) {
+    double vals[8];
+    for (int q = 0; q < 4; ++q) {
+      vals[2 * q] = acc[q].x;
+      vals[2 * q + 1] = acc[q].y;
+    }
+    block_reduce(vals, 2 * D, red);
+    if (threadIdx.x < 2 * D) atomicAdd(reinterpret_cast<double*>(gacc + op.grad_off) + threadIdx.x, vals[0]);
+  }
+}
+
+template <typename R>
+__global__ void __launch_bounds__(1024) k_tile_bwd(const typename CplxT<R>::T* __restrict__ x,
+                                                   typename CplxT<R>::T* __restrict__ lam, int nb, int batch,
+                                                   PassDesc pd, const TileOp* __restrict__ ops,
+                                                   const typename CplxT<R>::T* __restrict__ bmat, int64_t bmat_stride,
+                                                   const int* __restrict__ perms, double2* gacc, int64_t grad_stride) {
+  using C = typename CplxT<R>::T;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int t = pd.t, c = pd.c;
+  C* sx = reinterpret_cast<C*>(smem_raw);
+  C* sl = sx + (1 << t);
+  double* red = reinterpret_cast<double*>(sl + (1 << t));
+  uint32_t* tbl = reinterpret_cast<uint32_t*>(red + 32 * kRedSlots);
+  fill_table(tbl, pd);
+  const int64_t tiles_per = 1LL << (nb - t);
+  const int64_t ntiles = tiles_per * batch;
+  const uint64_t full = (nb >= 64) ? ~0ULL : ((1ULL << nb) - 1);
+  const uint64_t outer_mask = full & ~pd.tile_mask;
+  for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int64_t inst = tile >> (nb - t);
+    const uint64_t ti = static_cast<uint64_t>(tile) & static_cast<uint64_t>(tiles_per - 1);
+    const uint64_t o = (inst << nb) + pdep64(ti, outer_mask);
+    const C* bm = bmat + inst * bmat_stride;
+    double2* ga = gacc ? gacc + inst * grad_stride : nullptr;
+    __syncthreads();
+    tile_load(sx, x + o, tbl, t, c);
+    tile_load(sl, lam + o, tbl, t, c);
+    __syncthreads();
+    for (int oi = pd.op_end - 1; oi >= pd.op_begin; --oi) {
+      TileOp op = ops[oi];
+      if (!ga) op.grad_off = -1;
+      switch (op.kind) {
+        case BK_DENSE:
+          switch (op.kt) {
+            case 1: bwd_dense<C, 1>(sx, sl, t, op, bm + op.mat_off, ga, red); break;
+            case 2: bwd_dense<C, 2>(sx, sl, t, op, bm + op.mat_off, ga, red); break;
+            default: bwd_dense_wide<C>(sx, sl, t, op, bm + op.mat_off, ga); break;
+          }
+          break;
+        case BK_DIAG: bwd_diag<C>(sx, sl, t, op, bm + op.mat_off, ga, red); break;
+        default: tile_apply<C>(sl, t, op, bm, perms, true); break;
+      }
+      __syncthreads();
+    }
+    tile_store(sl, lam + o, tbl, t, c);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// block matrices: fuse each block's prims in float64, round to the run dtype
+// ---------------------------------------------------------------------------
+template <typename R>
+__global__ void k_prep(const DevBlock* __restrict__ blocks, int nblocks, const DevPrim* __restrict__ prims,
+                       const DevOp* __restrict__ ops, const double* __restrict__ angles, int n_angles,
+                       const double2* __restrict__ mats, int n_mats, const double2* __restrict__ cpool,
+                       typename CplxT<R>::T* __restrict__ bmat, int64_t bmat_stride, double2* scratch,
+                       int64_t scratch_stride, int batch) {
+  using C = typename CplxT<R>::T;
+  const int64_t idx = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (idx >= static_cast<int64_t>(batch) * nblocks) return;
+  const int inst = static_cast<int>(idx / nblocks), b = static_cast<int>(idx % nblocks);
+  const DevBlock blk = blocks[b];
+  if (blk.kind == BK_PERM) return;
+  const double* ang = angles ? angles + static_cast<int64_t>(inst) * n_angles : nullptr;
+  const double2* mt = mats ? mats + static_cast<int64_t>(inst) * n_mats : nullptr;
+  const int d = 1 << blk.k;
+  double2 la[16], lb[16], lc[16];
+  double2 *acc = la, *pm = lb, *tmp = lc;
+  if (blk.k > 2) {
+    double2* sc = scratch + inst * scratch_stride + blk.scratch_off;
+    acc = sc;
+    pm = sc + d * d;
+    tmp = sc + 2 * d * d;
+  }
+  prim_matrix(prims[blk.prim_begin], ops, ang, mt, cpool, acc, -1, tmp);
+  for (int p = blk.prim_begin + 1; p < blk.prim_end; ++p) {
+    prim_matrix(prims[p], ops, ang, mt, cpool, pm, -1, tmp);
+    m_mul(pm, acc, tmp, d);
+    m_copy(tmp, acc, d);
+  }
+  C* out = bmat + inst * bmat_stride + blk.mat_off;
+  const int base = d - blk.d;
+  if (blk.kind == BK_DIAG) {
+    for (int i = 0; i < blk.d; ++i) {
+      const double2 v = acc[(base + i) * d + base + i];
+      out[i] = cmake<C>(v.x, v.y);
+    }
+  } else {
+    for (int i = 0; i < blk.d; ++i)
+      for (int j = 0; j < blk.d; ++j) {
+        const double2 v = acc[(base + i) * d + base + j];
+        out[i * blk.d + j] = cmake<C>(v.x, v.y);
+      }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// chain rule: block cotangents -> per-prim cotangents -> angles / matrices
+// ---------------------------------------------------------------------------
+__global__ void k_chain(const DevBlock* __restrict__ blocks, int nblocks, const DevPrim* __restrict__ prims,
+                        const DevOp* __restrict__ ops, const double* __restrict__ angles, int n_angles,
+                        const double2* __restrict__ mats, int n_mats, const double2* __restrict__ cpool,
+                        const double2* __restrict__ gacc, int64_t grad_stride, double2* scratch,
+                        int64_t scratch_stride, int batch, double* grad_angles, double2* grad_mats) {
+  const int64_t idx = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (idx >= static_cast<int64_t>(batch) * nblocks) return;
+  const int inst = static_cast<int>(idx / nblocks), b = static_cast<int>(idx % nblocks);
+  const DevBlock blk = blocks[b];
+  if (blk.grad_off < 0) return;
+  const double* ang = angles ? angles + static_cast<int64_t>(inst) * n_angles : nullptr;
+  const double2* mt = mats ? mats + static_cast<int64_t>(inst) * n_mats : nullptr;
+  const double2* ga = gacc + inst * grad_stride + blk.grad_off;
+  const int d = 1 << blk.k;
+  double2 l0[16], l1[16], l2[16], l3[16], l4[16], l5[16];
+  double2 *Gb = l0, *A = l1, *B = l2, *P = l3, *T = l4, *T2 = l5;
+  if (blk.k > 2) {
+    double2* sc = scratch + inst * scratch_stride + blk.scratch_off;
+    Gb = sc; A = sc + d * d; B = sc + 2 * d * d; P = sc + 3 * d * d; T = sc + 4 * d * d; T2 = sc + 5 * d * d;
+  }
+  m_zero(Gb, d);
+  const int base = d - blk.d;
+  if (blk.kind == BK_DIAG) {
+    for (int i = 0; i < blk.d; ++i) Gb[(base + i) * d + base + i] = ga[i];
+  } else {
+    for (int i = 0; i < blk.d; ++i)
+      for (int j = 0; j < blk.d; ++j) Gb[(base + i) * d + base + j] = ga[i * blk.d + j];
+  }
+  const int m = blk.prim_end - blk.prim_begin;
+  for (int i = 0; i < m; ++i) {
+    const DevPrim p = prims[blk.prim_begin + i];
+    if (p.op < 0 || p.form == PF_CONST) continue;
+    const DevOp op = ops[p.op];
+    if (!op.grad) continue;
+    if (op.kind != JQ_K_MATRIX && op.n_angles == 0) continue;
+    // B = P_{i-1} ... P_0
+    m_identity(B, d);
+    for (int q = 0; q < i; ++q) {
+      prim_matrix(prims[blk.prim_begin + q], ops, ang, mt, cpool, P, -1, T2);
+      m_mul(P, B, T, d);
+      m_copy(T, B, d);
+    }
+    // A = P_{m-1} ... P_{i+1}
+    m_identity(A, d);
+    for (int q = i + 1; q < m; ++q) {
+      prim_matrix(prims[blk.prim_begin + q], ops, ang, mt, cpool, P, -1, T2);
+      m_mul(P, A, T, d);
+      m_copy(T, A, d);
+    }
+    // grad_P = A^dagger Gb B^dagger
+    m_mul_ah(A, Gb, T, d);
+    m_mul_bh(T, B, A, d);  // A now holds grad_P
+    if (op.kind == JQ_K_MATRIX) {
+      if (!grad_mats) continue;
+      double2* gm = grad_mats + static_cast<int64_t>(inst) * n_mats + op.mat_slot;
+      const int du = 1 << op.k;
+      if (p.form == PF_U || p.form == PF_CONJ) {
+        const double sgn = (p.form == PF_CONJ) ? -1.0 : 1.0;
+        if (op.mat_is_diag) {
+          for (int q = 0; q < du; ++q) {
+            atomicAdd(&gm[q].x, A[q * d + q].x);
+            atomicAdd(&gm[q].y, sgn * A[q * d + q].y);
+          }
+        } else {
+          for (int q = 0; q < du * du; ++q) {
+            atomicAdd(&gm[q].x, A[q].x);
+            atomicAdd(&gm[q].y, sgn * A[q].y);
+          }
+        }
+      } else if (p.form == PF_KRON) {
+        // S = U (x) conj U: grad_U = X1 + X2 with
+        // X1_ab = sum_cd G[ac,bd] U_cd, X2_cd = sum_ab conj(G[ac,bd]) U_ab
+        double2 U[4];
+        op_matrix(op, ang, mt, U, -1, T2);
+        double2 gu[4];
+        for (int q = 0; q < 4; ++q) gu[q] = make_double2(0, 0);
+        for (int a = 0; a < 2; ++a)
+          for (int bb = 0; bb < 2; ++bb)
+            for (int c = 0; c < 2; ++c)
+              for (int e = 0; e < 2; ++e) {
+                const double2 g = A[(a * 2 + c) * 4 + (bb * 2 + e)];
+                gu[a * 2 + bb] = cfma(g, U[c * 2 + e], gu[a * 2 + bb]);
+                gu[c * 2 + e] = cfma(cconj(g), U[a * 2 + bb], gu[c * 2 + e]);
+              }
+        if (op.mat_is_diag) {
+          atomicAdd(&gm[0].x, gu[0].x); atomicAdd(&gm[0].y, gu[0].y);
+          atomicAdd(&gm[1].x, gu[3].x); atomicAdd(&gm[1].y, gu[3].y);
+        } else {
+          for (int q = 0; q < 4; ++q) { atomicAdd(&gm[q].x, gu[q].x); atomicAdd(&gm[q].y, gu[q].y); }
+        }
+      }
+      continue;
+    }
+    if (!grad_angles) continue;
+    for (int j = 0; j < op.n_angles; ++j) {
+      prim_matrix(p, ops, ang, mt, cpool, P, j, T2);
+      const double g = m_inner_re(A, P, d);
+      atomicAdd(&grad_angles[static_cast<int64_t>(inst) * n_angles + op.angle_slot + j], g);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// state initialisation and measurements
+// ---------------------------------------------------------------------------
+template <typename R>
+__global__ void k_init(typename CplxT<R>::T* state, int64_t elems, int batch, const typename CplxT<R>::T* init,
+                       int64_t init_elems, int init_batched, int pure_density) {
+  using C = typename CplxT<R>::T;
+  const int64_t total = elems * batch;
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < total;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t inst = i / elems, j = i - inst * elems;
+    C v;
+    if (!init) {
+      v = cmake<C>(j == 0 ? 1.0 : 0.0, 0.0);
+    } else {
+      const C* src = init + (init_batched ? inst * init_elems : 0);
+      if (!pure_density) {
+        v = src[j];
+      } else {
+        // rho = psi psi^dagger (jaqsi/simulation.py:470-471)
+        const int64_t r = j / init_elems, c = j - r * init_elems;
+        v = cmulc(src[r], src[c]);
+      }
+    }
+    state[i] = v;
+  }
+}
+
+template <typename R>
+__global__ void k_probs_sv(const typename CplxT<R>::T* psi, R* out, int64_t total) {
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < total;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const auto a = psi[i];
+    out[i] = a.x * a.x + a.y * a.y;
+  }
+}
+
+template <typename R>
+__global__ void k_probs_dm(const typename CplxT<R>::T* rho, R* out, int64_t dim, int batch) {
+  const int64_t total = dim * batch;
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < total;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t inst = i / dim, j = i - inst * dim;
+    out[i] = rho[inst * dim * dim + j * dim + j].x;
+  }
+}
+
+template <typename R>
+__global__ void k_outer(const typename CplxT<R>::T* psi, typename CplxT<R>::T* out, int64_t dim, int batch) {
+  const int64_t total = dim * dim * batch;
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < total;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t inst = i / (dim * dim), e = i - inst * dim * dim;
+    const int64_t r = e / dim, c = e - r * dim;
+    out[i] = cmulc(psi[inst * dim + r], psi[inst * dim + c]);
+  }
+}
+
+// i^ny * w, real part
+__device__ __forceinline__ double re_iy(int ny, double2 w) {
+  switch (ny & 3) {
+    case 0: return w.x;
+    case 1: return -w.y;
+    case 2: return -w.x;
+    default: return w.y;
+  }
+}
+__device__ __forceinline__ double2 mul_iy(int ny, double2 w) {
+  switch (ny & 3) {
+    case 0: return w;
+    case 1: return make_double2(-w.y, w.x);
+    case 2: return make_double2(-w.x, -w.y);
+    default: return make_double2(w.y, -w.x);
+  }
+}
+
+constexpr int kObsChunk = 16;
+
+// <psi| coeff P |psi> for up to kObsChunk Pauli words, float64 accumulation.
+template <typename R>
+__global__ void k_expval_pauli_sv(const typename CplxT<R>::T* psi, int64_t dim, const DevObs* obs, int o_begin,
+                                  int o_cnt, double* out, int n_obs) {
+  __shared__ double red[32 * kRedSlots];
+  const int inst = blockIdx.y;
+  const auto* p = psi + static_cast<int64_t>(inst) * dim;
+  double acc[kObsChunk];
+#pragma unroll
+  for (int o = 0; o < kObsChunk; ++o) acc[o] = 0.0;
+  for (int64_t j = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < dim;
+       j += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const double2 a = to_d2(p[j]);
+#pragma unroll
+    for (int o = 0; o < kObsChunk; ++o) {
+      if (o < o_cnt) {
+        const DevObs ob = obs[o_begin + o];
+        const int64_t jx = j ^ static_cast<int64_t>(ob.x_mask);
+        // (P psi)_j = phase(j ^ x) psi_{j ^ x}
+        const double sign = (__popcll(static_cast<uint64_t>(jx) & ob.z_mask) & 1) ? -1.0 : 1.0;
+        if (ob.x_mask == 0) {
+          acc[o] += ob.coeff * sign * (a.x * a.x + a.y * a.y);
+        } else {
+          const double2 bv = to_d2(p[jx]);
+          const double2 w = cmul(cconj(a), bv);
+          acc[o] += ob.coeff * sign * re_iy(ob.n_y, w);
+        }
+      }
+    }
+  }
+  block_reduce(acc, o_cnt, red);
+  if (threadIdx.x < o_cnt) atomicAdd(&out[static_cast<int64_t>(inst) * n_obs + o_begin + threadIdx.x], acc[0]);
+}
+
+// <psi|O|psi> for one dense Hermitian observable on k wires.
+template <typename R>
+__global__ void k_expval_dense_sv(const typename CplxT<R>::T* psi, int n, const DevObs* obs, int oi,
+                                  const double2* pool, double* out, int n_obs) {
+  __shared__ double red[32 * kRedSlots];
+  const int inst = blockIdx.y;
+  const DevObs ob = obs[oi];
+  const int k = ob.k, D = 1 << k;
+  const int64_t dim = 1LL << n;
+  const auto* p = psi + static_cast<int64_t>(inst) * dim;
+  const double2* O = pool + ob.mat_off;
+  uint64_t fix = 0;
+  for (int i = 0; i < k; ++i) fix |= 1ULL << ob.bits[i];
+  const int64_t groups = dim >> k;
+  double acc = 0.0;
+  for (int64_t g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; g < groups;
+       g += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const uint64_t base = pdep64(static_cast<uint64_t>(g), ((dim - 1) & ~fix));
+    for (int a = 0; a < D; ++a) {
+      uint64_t ia = base;
+      for (int i = 0; i < k; ++i)
+        if ((a >> (k - 1 - i)) & 1) ia |= 1ULL << ob.bits[i];
+      const double2 va = to_d2(p[ia]);
+      double2 row = make_double2(0, 0);
+      for (int bcol = 0; bcol < D; ++bcol) {
+        uint64_t ib = base;
+        for (int i = 0; i < k; ++i)
+          if ((bcol >> (k - 1 - i)) & 1) ib |= 1ULL << ob.bits[i];
+        row = cfma(O[a * D + bcol], to_d2(p[ib]), row);
+      }
+      acc += va.x * row.x + va.y * row.y;
+    }
+  }
+  block_reduce(&acc, 1, red);
+  if (threadIdx.x == 0) atomicAdd(&out[static_cast<int64_t>(inst) * n_obs + oi], acc);
+}
+
+// Tr(coeff P rho) = coeff sum_k phase(k) rho[k][k ^ x]
+template <typename R>
+__global__ void k_expval_pauli_dm(const typename CplxT<R>::T* rho, int64_t dim, const DevObs* obs, int o_begin,
+                                  int o_cnt, double* out, int n_obs) {
+  __shared__ double red[32 * kRedSlots];
+  const int inst = blockIdx.y;
+  const auto* p = rho + static_cast<int64_t>(inst) * dim * dim;
+  double acc[kObsChunk];
+#pragma unroll
+  for (int o = 0; o < kObsChunk; ++o) acc[o] = 0.0;
+  for (int64_t j = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < dim;
+       j += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+#pragma unroll
+    for (int o = 0; o < kObsChunk; ++o) {
+      if (o < o_cnt) {
+        const DevObs ob = obs[o_begin + o];
+        const int64_t jx = j ^ static_cast<int64_t>(ob.x_mask);
+        const double sign = (__popcll(static_cast<uint64_t>(j) & ob.z_mask) & 1) ? -1.0 : 1.0;
+        const double2 v = to_d2(p[j * dim + jx]);
+        acc[o] += ob.coeff * sign * re_iy(ob.n_y, v);
+      }
+    }
+  }
+  block_reduce(acc, o_cnt, red);
+  if (threadIdx.x < o_cnt) atomicAdd(&out[static_cast<int64_t>(inst) * n_obs + o_begin + threadIdx.x], acc[0]);
+}
+
+// Tr(O rho) = sum_ab O_ab sum_rest rho[(b,rest)][(a,rest)]
+template <typename R>
+__global__ void k_expval_dense_dm(const typename CplxT<R>::T* rho, int n, const DevObs* obs, int oi,
+                                  const double2* pool, double* out, int n_obs) {
+  __shared__ double red[32 * kRedSlots];
+  const int inst = blockIdx.y;
+  const DevObs ob = obs[oi];
+  const int k = ob.k, D = 1 << k;
+  const int64_t dim = 1LL << n;
+  const auto* p = rho + static_cast<int64_t>(inst) * dim * dim;
+  const double2* O = pool + ob.mat_off;
+  uint64_t fix = 0;
+  for (int i = 0; i < k; ++i) fix |= 1ULL << ob.bits[i];
+  const int64_t groups = dim >> k;
+  double acc = 0.0;
+  for (int64_t g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; g < groups;
+       g += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const uint64_t base = pdep64(static_cast<uint64_t>(g), ((dim - 1) & ~fix));
+    for (int a = 0; a < D; ++a) {
+      uint64_t ia = base;
+      for (int i = 0; i < k; ++i)
+        if ((a >> (k - 1 - i)) & 1) ia |= 1ULL << ob.bits[i];
+      for (int bcol = 0; bcol < D; ++bcol) {
+        uint64_t ib = base;
+        for (int i = 0; i < k; ++i)
+          if ((bcol >> (k - 1 - i)) & 1) ib |= 1ULL << ob.bits[i];
+        const double2 w = cmul(O[a * D + bcol], to_d2(p[ib * dim + ia]));
+        acc += w.x;
+      }
+    }
+  }
+  block_reduce(&acc, 1, red);
+  if (threadIdx.x == 0) atomicAdd(&out[static_cast<int64_t>(inst) * n_obs + oi], acc);
+}
+
+// ---------------------------------------------------------------------------
+// seeds of the reverse pass (lam = dL/dRe + i dL/dIm of the final state)
+// ---------------------------------------------------------------------------
+// statevector expval: lam = 2 sum_o ct_o O_o psi
+template <typename R>
+__global__ void k_seed_expval_sv(const typename CplxT<R>::T* psi, typename CplxT<R>::T* lam, int n, int batch,
+                                 const DevObs* obs, int n_obs, const double2* pool, const double* ct) {
+  using C = typename CplxT<R>::T;
+  const int64_t dim = 1LL << n;
+  const int64_t total = dim * batch;
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < total;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t inst = i / dim, j = i - inst * dim;
+    const C* p = psi + inst * dim;
+    double2 acc = make_double2(0, 0);
+    for (int o = 0; o < n_obs; ++o) {
+      const DevObs ob = obs[o];
+      const double w = 2.0 * ct[inst * n_obs + o];
+      if (w == 0.0) continue;
+      if (ob.kind == JQ_OBS_PAULI) {
+        const int64_t jx = j ^ static_cast<int64_t>(ob.x_mask);
+        const double sign = (__popcll(static_cast<uint64_t>(jx) & ob.z_mask) & 1) ? -1.0 : 1.0;
+        const double2 v = mul_iy(ob.n_y, to_d2(p[jx]));
+        acc.x += w * ob.coeff * sign * v.x;
+        acc.y += w * ob.coeff * sign * v.y;
+      } else {
+        const int k = ob.k, D = 1 << k;
+        int a = 0;
+        uint64_t rest = static_cast<uint64_t>(j);
+        for (int q = 0; q < k; ++q) {
+          a = (a << 1) | static_cast<int>((j >> ob.bits[q]) & 1);
+          rest &= ~(1ULL << ob.bits[q]);
+        }
+        double2 row = make_double2(0, 0);
+        for (int bcol = 0; bcol < D; ++bcol) {
+          uint64_t ib = rest;
+          for (int q = 0; q < k; ++q)
+            if ((bcol >> (k - 1 - q)) & 1) ib |= 1ULL << ob.bits[q];
+          row = cfma(pool[ob.mat_off + a * D + bcol], to_d2(p[ib]), row);
+        }
+        acc.x += w * row.x;
+        acc.y += w * row.y;
+      }
+    }
+    lam[i] = cmake<C>(acc.x, acc.y);
+  }
+}
+
+// statevector probs: lam_j = 2 ct_j psi_j
+template <typename R>
+__global__ void k_seed_probs_sv(const typename CplxT<R>::T* psi, typename CplxT<R>::T* lam, const R* ct,
+                                int64_t total) {
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < total;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const R w = 2 * ct[i];
+    auto a = psi[i];
+    a.x *= w;
+    a.y *= w;
+    lam[i] = a;
+  }
+}
+
+// pure density output rho = psi psi^dagger: lam = (G + G^dagger) psi
+template <typename R>
+__global__ void k_seed_density_sv(const typename CplxT<R>::T* psi, typename CplxT<R>::T* lam,
+                                  const typename CplxT<R>::T* G, int64_t dim, int batch) {
+  using C = typename CplxT<R>::T;
+  const int64_t total = dim * batch;
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < total;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t inst = i / dim, r = i - inst * dim;
+    const C* g = G + inst * dim * dim;
+    const C* p = psi + inst * dim;
+    double2 acc = make_double2(0, 0);
+    for (int64_t c = 0; c < dim; ++c) {
+      const double2 m = cadd(to_d2(g[r * dim + c]), cconj(to_d2(g[c * dim + r])));
+      acc = cfma(m, to_d2(p[c]), acc);
+    }
+    lam[i] = cmake<C>(acc.x, acc.y);
+  }
+}
+
+// density expval: lam[r][c] = sum_o ct_o O_o[r][c]
+template <typename R>
+__global__ void k_seed_expval_dm(typename CplxT<R>::T* lam, int n, int batch, const DevObs* obs, int n_obs,
+                                 const double2* pool, const double* ct) {
+  using C = typename CplxT<R>::T;
+  const int64_t dim = 1LL << n, sz = dim * dim;
+  const int64_t total = sz * batch;
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < total;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t inst = i / sz, e = i - inst * sz;
+    const uint64_t r = static_cast<uint64_t>(e / dim), c = static_cast<uint64_t>(e - (e / dim) * dim);
+    double2 acc = make_double2(0, 0);
+    for (int o = 0; o < n_obs; ++o) {
+      const DevObs ob = obs[o];
+      const double w = ct[inst * n_obs + o];
+      if (w == 0.0) continue;
+      if (ob.kind == JQ_OBS_PAULI) {
+        if ((r ^ c) != ob.x_mask) continue;
+        const double sign = (__popcll(c & ob.z_mask) & 1) ? -1.0 : 1.0;
+        const double2 v = mul_iy(ob.n_y, make_double2(w * ob.coeff * sign, 0.0));
+        acc = cadd(acc, v);
+      } else {
+        uint64_t fix = 0;
+        int a = 0, bcol = 0;
+        for (int q = 0; q < ob.k; ++q) {
+          fix |= 1ULL << ob.bits[q];
+          a = (a << 1) | static_cast<int>((r >> ob.bits[q]) & 1);
+          bcol = (bcol << 1) | static_cast<int>((c >> ob.bits[q]) & 1);
+        }
+        if ((r & ~fix) != (c & ~fix)) continue;
+        const double2 v = pool[ob.mat_off + a * (1 << ob.k) + bcol];
+        acc.x += w * v.x;
+        acc.y += w * v.y;
+      }
+    }
+    lam[i] = cmake<C>(acc.x, acc.y);
+  }
+}
+
+// density probs: lam = diag(ct)
+template <typename R>
+__global__ void k_seed_probs_dm(typename CplxT<R>::T* lam, const R* ct, int64_t dim, int batch) {
+  using C = typename CplxT<R>::T;
+  const int64_t sz = dim * dim, total = sz * batch;
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < total;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t inst = i / sz, e = i - inst * sz;
+    const int64_t r = e / dim, c = e - r * dim;
+    lam[i] = cmake<C>(r == c ? static_cast<double>(ct[inst * dim + r]) : 0.0, 0.0);
+  }
+}
+
+// cotangent of psi0 when rho0 = psi0 psi0^dagger: (L + L^dagger) psi0
+template <typename R>
+__global__ void k_grad_init_dm(const typename CplxT<R>::T* lam, const typename CplxT<R>::T* init, int init_batched,
+                               typename CplxT<R>::T* out, int64_t dim, int batch) {
+  using C = typename CplxT<R>::T;
+  const int64_t total = dim * batch;
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < total;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t inst = i / dim, r = i - inst * dim;
+    const C* L = lam + inst * dim * dim;
+    const C* p = init + (init_batched ? inst * dim : 0);
+    double2 acc = make_double2(0, 0);
+    for (int64_t c = 0; c < dim; ++c) {
+      const double2 m = cadd(to_d2(L[r * dim + c]), cconj(to_d2(L[c * dim + r])));
+      acc = cfma(m, to_d2(p[c]), acc);
+    }
+    out[i] = cmake<C>(acc.x, acc.y);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+#define JQ_CUDA(expr)                                                                     \
+  do {                                                                                    \
+    cudaError_t _e = (expr);                                                              \
+    if (_e != cudaSuccess) {                                                              \
+      set_error(std::string("CUDA error: ") + cudaGetErrorString(_e) + " at " #expr);     \
+      return JQ_ECUDA;                                                                    \
+    }                                                                                     \
+  } while (0)
+
+int g_sm_count = 0;
+
+int sm_count() {
+  if (g_sm_count == 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&g_sm_count, cudaDevAttrMultiProcessorCount, dev);
+    if (g_sm_count <= 0) g_sm_count = 148;
+  }
+  return g_sm_count;
+}
+
+std::mutex g_upload_mu;
+
+template <typename T>
+int upload(const std::vector<T>& v, T** dst) {
+  *dst = nullptr;
+  if (v.empty()) return JQ_OK;
+  JQ_CUDA(cudaMalloc(reinterpret_cast<void**>(dst), v.size() * sizeof(T)));
+  JQ_CUDA(cudaMemcpy(*dst, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+  return JQ_OK;
+}
+
+int device_tables(const jq_plan* cplan, const DeviceTables** out) {
+  jq_plan* plan = const_cast<jq_plan*>(cplan);
+  int dev = 0;
+  JQ_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lock(g_upload_mu);
+  for (const DeviceTables& t : plan->dev)
+    if (t.device == dev) { *out = &t; return JQ_OK; }
+  DeviceTables t;
+  t.device = dev;
+  int rc;
+  if ((rc = upload(plan->ops, &t.ops))) return rc;
+  if ((rc = upload(plan->prims, &t.prims))) return rc;
+  if ((rc = upload(plan->blocks, &t.blocks))) return rc;
+  if ((rc = upload(plan->fwd.ops, &t.fwd_ops))) return rc;
+  if ((rc = upload(plan->adj.ops, &t.adj_ops))) return rc;
+  if ((rc = upload(plan->const_pool, &t.const_pool))) return rc;
+  if ((rc = upload(plan->perm_pool, &t.perm_pool))) return rc;
+  if ((rc = upload(plan->obs_pool, &t.obs_pool))) return rc;
+  DevObs* od = nullptr;
+  if ((rc = upload(plan->obs, &od))) return rc;
+  t.obs_desc = od;
+  TileOp* bo = nullptr;
+  if ((rc = upload(plan->bwd.ops, &bo))) return rc;
+  t.bwd_ops = bo;
+  plan->dev.push_back(t);
+  *out = &plan->dev.back();
+  return JQ_OK;
+}
+
+size_t align256(size_t x) { return (x + 255) & ~static_cast<size_t>(255); }
+
+struct WsLayout {
+  size_t bmat = 0, scratch = 0, lam = 0, psi = 0, gacc = 0, ckpt = 0, seg = 0, work = 0, total = 0;
+  int64_t n_ckpt = 0, seg_len = 0;
+};
+
+WsLayout layout(const jq_plan* plan, int batch, int mode_grad /*0 fwd, 1 adjoint, 2 ckpt*/) {
+  WsLayout L;
+  const size_t elem = plan->dtype == JQ_C64 ? 8 : 16;
+  const size_t state = static_cast<size_t>(plan->state_elems) * elem * batch;
+  size_t off = 0;
+  L.bmat = off;
+  off += align256(static_cast<size_t>(plan->bmat_stride) * elem * batch);
+  L.scratch = off;
+  off += align256(static_cast<size_t>(plan->scratch_stride) * 16 * batch);
+  if (mode_grad >= 1) {
+    L.lam = off;
+    off += align256(state);
+    L.gacc = off;
+    off += align256(static_cast<size_t>(plan->grad_stride) * 16 * batch);
+  }
+  if (mode_grad == 1) {
+    L.psi = off;
+    off += align256(state);
+  }
+  if (mode_grad == 2) {
+    const int64_t P = static_cast<int64_t>(plan->bwd.passes.size());
+    int64_t S = plan->ckpt_stride > 0 ? plan->ckpt_stride : static_cast<int64_t>(std::ceil(std::sqrt(static_cast<double>(std::max<int64_t>(P, 1)))));
+    S = std::max<int64_t>(1, S);
+    L.seg_len = S;
+    L.n_ckpt = (P + S - 1) / S;
+    L.work = off;
+    off += align256(state);
+    L.ckpt = off;
+    off += align256(state) * static_cast<size_t>(std::max<int64_t>(L.n_ckpt, 1));
+    L.seg = off;
+    off += align256(state) * static_cast<size_t>(S);
+  }
+  L.total = off;
+  return L;
+}
+
+int grid_for(int64_t work, int threads) {
+  int64_t g = (work + threads - 1) / threads;
+  const int64_t cap = static_cast<int64_t>(sm_count()) * 16;
+  return static_cast<int>(std::max<int64_t>(1, std::min(g, cap)));
+}
+
+template <typename R>
+size_t tile_smem(const PassDesc& pd, int n_tiles_in_smem) {
+  const size_t elem = sizeof(typename CplxT<R>::T);
+  size_t s = (static_cast<size_t>(n_tiles_in_smem) << pd.t) * elem;
+  if (n_tiles_in_smem == 2) s += 32 * kRedSlots * sizeof(double);
+  s += (static_cast<size_t>(1) << (pd.t - pd.c)) * sizeof(uint32_t);
+  return s;
+}
+
+template <typename R>
+int set_smem_attrs() {
+  static bool done = false;
+  if (done) return JQ_OK;
+  const int max_smem = 227 * 1024;
+  JQ_CUDA(cudaFuncSetAttribute(k_tile_fwd<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem));
+  JQ_CUDA(cudaFuncSetAttribute(k_tile_adj<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem));
+  JQ_CUDA(cudaFuncSetAttribute(k_tile_bwd<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem));
+  done = true;
+  return JQ_OK;
+}
+
+template <typename K>
+int ctas_for(K kernel, int threads, size_t smem, int64_t ntiles) {
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem);
+  if (per_sm < 1) per_sm = 1;
+  int64_t cap = static_cast<int64_t>(sm_count()) * per_sm;
+  return static_cast<int>(std::max<int64_t>(1, std::min(ntiles, cap)));
+}
+
+// Run passes [p0, p1) of a schedule over `state` (batch instances).
+template <typename R>
+int run_passes(const jq_plan* plan, const Schedule& sch, const TileOp* dops, const DeviceTables* T,
+               typename CplxT<R>::T* state, int batch, const typename CplxT<R>::T* bmat, size_t p0, size_t p1,
+               cudaStream_t st) {
+  for (size_t p = p0; p < p1; ++p) {
+    const PassDesc& pd = sch.passes[p];
+    if (pd.op_end == pd.op_begin) continue;
+    const size_t smem = tile_smem<R>(pd, 1);
+    const int64_t ntiles = (1LL << (plan->n_bits - pd.t)) * batch;
+    const int ctas = ctas_for(k_tile_fwd<R>, plan->threads, smem, ntiles);
+    k_tile_fwd<R><<<ctas, plan->threads, smem, st>>>(state, plan->n_bits, batch, pd, dops, bmat, plan->bmat_stride,
+                                                      T->perm_pool);
+  }
+  JQ_CUDA(cudaGetLastError());
+  return JQ_OK;
+}
+
+template <typename R>
+int prep(const jq_plan* plan, const DeviceTables* T, int batch, const double* angles, const void* mats,
+         typename CplxT<R>::T* bmat, double2* scratch, cudaStream_t st) {
+  const int nbk = static_cast<int>(plan->blocks.size());
+  if (nbk == 0) return JQ_OK;
+  const int64_t work = static_cast<int64_t>(nbk) * batch;
+  const int threads = 128;
+  const int grid = static_cast<int>((work + threads - 1) / threads);
+  k_prep<R><<<grid, threads, 0, st>>>(T->blocks, nbk, T->prims, T->ops, angles, plan->n_angles,
+                                      reinterpret_cast<const double2*>(mats), plan->n_mats,
+                                      reinterpret_cast<const double2*>(T->const_pool), bmat, plan->bmat_stride,
+                                      scratch, plan->scratch_stride, batch);
+  JQ_CUDA(cudaGetLastError());
+  return JQ_OK;
+}
+
+template <typename R>
+int measure(const jq_plan* plan, const DeviceTables* T, int batch, int out_type, const typename CplxT<R>::T* state,
+            void* out, cudaStream_t st) {
+  using C = typename CplxT<R>::T;
+  const int n = plan->n_qubits;
+  const int64_t dim = 1LL << n;
+  const bool dm = plan->mode == JQ_DENSITY;
+  const int threads = 256;
+  if (out_type == JQ_OUT_STATE) return JQ_OK;
+  if (out_type == JQ_OUT_PROBS) {
+    if (dm) {
+      k_probs_dm<R><<<grid_for(dim * batch, threads), threads, 0, st>>>(state, static_cast<R*>(out), dim, batch);
+    } else {
+      k_probs_sv<R><<<grid_for(dim * batch, threads), threads, 0, st>>>(state, static_cast<R*>(out), dim * batch);
+    }
+  } else if (out_type == JQ_OUT_DENSITY) {
+    if (dm) return JQ_OK;  // the state is the density matrix
+    k_outer<R><<<grid_for(dim * dim * batch, threads), threads, 0, st>>>(state, static_cast<C*>(out), dim, batch);
+  } else if (out_type == JQ_OUT_EXPVAL) {
+    const int n_obs = static_cast<int>(plan->obs.size());
+    if (n_obs == 0) return JQ_OK;
+    double* o = static_cast<double*>(out);
+    JQ_CUDA(cudaMemsetAsync(o, 0, sizeof(double) * n_obs * batch, st));
+    const DevObs* od = static_cast<const DevObs*>(T->obs_desc);
+    const double2* pool = reinterpret_cast<const double2*>(T->obs_pool);
+    // Pauli observables in chunks; dense ones one launch each
+    int i = 0;
+    while (i < n_obs) {
+      if (plan->obs[i].kind == JQ_OBS_PAULI) {
+        int j = i;
+        while (j < n_obs && j - i < kObsChunk && plan->obs[j].kind == JQ_OBS_PAULI) ++j;
+        const int gx = std::max(1, std::min<int>(static_cast<int>((dim + threads - 1) / threads),
+                                                 std::max(1, 4 * sm_count() / std::max(batch, 1))));
+        dim3 grid(gx, batch);
+        if (dm) k_expval_pauli_dm<R><<<grid, threads, 0, st>>>(state, dim, od, i, j - i, o, n_obs);
+        else k_expval_pauli_sv<R><<<grid, threads, 0, st>>>(state, dim, od, i, j - i, o, n_obs);
+        i = j;
+      } else {
+        const int64_t groups = dim >> plan->obs[i].k;
+        const int gx = std::max(1, std::min<int>(static_cast<int>((groups + threads - 1) / threads),
+                                                 std::max(1, 4 * sm_count() / std::max(batch, 1))));
+        dim3 grid(gx, batch);
+        if (dm) k_expval_dense_dm<R><<<grid, threads, 0, st>>>(state, n, od, i, pool, o, n_obs);
+        else k_expval_dense_sv<R><<<grid, threads, 0, st>>>(state, n, od, i, pool, o, n_obs);
+        ++i;
+      }
+    }
+  } else {
+    set_error("unknown out_type");
+    return JQ_EINVAL;
+  }
+  JQ_CUDA(cudaGetLastError());
+  return JQ_OK;
+}
+
+template <typename R>
+int forward_impl(const jq_plan* plan, int batch, const double* angles, const void* mats, const void* init,
+                 int init_batched, int out_type, void* state, void* out, void* ws, size_t ws_bytes,
+                 cudaStream_t st) {
+  using C = typename CplxT<R>::T;
+  const DeviceTables* T = nullptr;
+  int rc = device_tables(plan, &T);
+  if (rc) return rc;
+  if ((rc = set_smem_attrs<R>())) return rc;
+  WsLayout L = layout(plan, batch, 0);
+  if (ws_bytes < L.total || (L.total > 0 && !ws)) {
+    set_error("workspace too small: need " + std::to_string(L.total) + " bytes");
+    return JQ_ENOMEM;
+  }
+  char* w = static_cast<char*>(ws);
+  C* bmat = reinterpret_cast<C*>(w + L.bmat);
+  double2* scratch = reinterpret_cast<double2*>(w + L.scratch);
+  if ((rc = prep<R>(plan, T, batch, angles, mats, bmat, scratch, st))) return rc;
+  C* S = static_cast<C*>(state);
+  const bool dm = plan->mode == JQ_DENSITY;
+  const int64_t dim = 1LL << plan->n_qubits;
+  k_init<R><<<grid_for(plan->state_elems * batch, 256), 256, 0, st>>>(
+      S, plan->state_elems, batch, static_cast<const C*>(init), dim, init_batched, dm && init ? 1 : 0);
+  JQ_CUDA(cudaGetLastError());
+  if ((rc = run_passes<R>(plan, plan->fwd, T->fwd_ops, T, S, batch, bmat, 0, plan->fwd.passes.size(), st))) return rc;
+  return measure<R>(plan, T, batch, out_type, S, out, st);
+}
+
+template <typename R>
+int seed_sv(const jq_plan* plan, const DeviceTables* T, int batch, int out_type, const typename CplxT<R>::T* psi,
+            const double* ct, const void* ct_state, typename CplxT<R>::T* lam, cudaStream_t st) {
+  using C = typename CplxT<R>::T;
+  const int64_t dim = 1LL << plan->n_qubits;
+  const int threads = 256;
+  switch (out_type) {
+    case JQ_OUT_EXPVAL:
+      k_seed_expval_sv<R><<<grid_for(dim * batch, threads), threads, 0, st>>>(
+          psi, lam, plan->n_qubits, batch, static_cast<const DevObs*>(T->obs_desc), static_cast<int>(plan->obs.size()),
+          reinterpret_cast<const double2*>(T->obs_pool), ct);
+      break;
+    case JQ_OUT_STATE:
+      JQ_CUDA(cudaMemcpyAsync(lam, ct_state, sizeof(C) * dim * batch, cudaMemcpyDeviceToDevice, st));
+      break;
+    case JQ_OUT_PROBS:
+      k_seed_probs_sv<R><<<grid_for(dim * batch, threads), threads, 0, st>>>(psi, lam, static_cast<const R*>(ct_state),
+                                                                             dim * batch);
+      break;
+    case JQ_OUT_DENSITY:
+      k_seed_density_sv<R><<<grid_for(dim * batch, threads), threads, 0, st>>>(psi, lam, static_cast<const C*>(ct_state),
+                                                                               dim, batch);
+      break;
+    default:
+      set_error("unknown out_type");
+      return JQ_EINVAL;
+  }
+  JQ_CUDA(cudaGetLastError());
+  return JQ_OK;
+}
+
+template <typename R>
+int seed_dm(const jq_plan* plan, const DeviceTables* T, int batch, int out_type, const double* ct,
+            const void* ct_state, typename CplxT<R>::T* lam, cudaStream_t st) {
+  using C = typename CplxT<R>::T;
+  const int64_t dim = 1LL << plan->n_qubits;
+  const int threads = 256;
+  switch (out_type) {
+    case JQ_OUT_EXPVAL:
+      k_seed_expval_dm<R><<<grid_for(dim * dim * batch, threads), threads, 0, st>>>(
+          lam, plan->n_qubits, batch, static_cast<const DevObs*>(T->obs_desc), static_cast<int>(plan->obs.size()),
+          reinterpret_cast<const double2*>(T->obs_pool), ct);
+      break;
+    case JQ_OUT_STATE:
+    case JQ_OUT_DENSITY:
+      JQ_CUDA(cudaMemcpyAsync(lam, ct_state, sizeof(C) * dim * dim * batch, cudaMemcpyDeviceToDevice, st));
+      break;
+    case JQ_OUT_PROBS:
+      k_seed_probs_dm<R><<<grid_for(dim * dim * batch, threads), threads, 0, st>>>(lam, static_cast<const R*>(ct_state),
+                                                                                  dim, batch);
+      break;
+    default:
+      set_error("unknown out_type");
+      return JQ_EINVAL;
+  }
+  JQ_CUDA(cudaGetLastError());
+  return JQ_OK;
+}
+
+template <typename R>
+int chain(const jq_plan* plan, const DeviceTables* T, int batch, const double* angles, const void* mats,
+          const double2* gacc, double2* scratch, double* grad_angles, void* grad_mats, cudaStream_t st) {
+  if (grad_angles && plan->n_angles > 0)
+    JQ_CUDA(cudaMemsetAsync(grad_angles, 0, sizeof(double) * plan->n_angles * batch, st));
+  if (grad_mats && plan->n_mats > 0)
+    JQ_CUDA(cudaMemsetAsync(grad_mats, 0, 16 * static_cast<size_t>(plan->n_mats) * batch, st));
+  const int nbk = static_cast<int>(plan->blocks.size());
+  if (nbk == 0 || plan->grad_stride == 0) return JQ_OK;
+  const int64_t work = static_cast<int64_t>(nbk) * batch;
+  const int threads = 64;
+  k_chain<<<static_cast<int>((work + threads - 1) / threads), threads, 0, st>>>(
+      T->blocks, nbk, T->prims, T->ops, angles, plan->n_angles, reinterpret_cast<const double2*>(mats), plan->n_mats,
+      reinterpret_cast<const double2*>(T->const_pool), gacc, plan->grad_stride, scratch, plan->scratch_stride, batch,
+      grad_angles, static_cast<double2*>(grad_mats));
+  JQ_CUDA(cudaGetLastError());
+  return JQ_OK;
+}
+
+template <typename R>
+int adjoint_impl(const jq_plan* plan, int batch, const double* angles, const void* mats, const void* state,
+                 int out_type, const double* ct, const void* ct_state, double* grad_angles, void* grad_mats,
+                 void* grad_init, void* ws, size_t ws_bytes, cudaStream_t st) {
+  using C = typename CplxT<R>::T;
+  if (plan->mode != JQ_STATEVECTOR || !plan->unitary) {
+    set_error("jq_adjoint needs a unitary statevector plan; use jq_backward");
+    return JQ_EINVAL;
+  }
+  const DeviceTables* T = nullptr;
+  int rc = device_tables(plan, &T);
+  if (rc) return rc;
+  if ((rc = set_smem_attrs<R>())) return rc;
+  WsLayout L = layout(plan, batch, 1);
+  if (ws_bytes < L.total || !ws) {
+    set_error("workspace too small: need " + std::to_string(L.total) + " bytes");
+    return JQ_ENOMEM;
+  }
+  char* w = static_cast<char*>(ws);
+  C* bmat = reinterpret_cast<C*>(w + L.bmat);
+  double2* scratch = reinterpret_cast<double2*>(w + L.scratch);
+  C* lam = reinterpret_cast<C*>(w + L.lam);
+  C* psi = reinterpret_cast<C*>(w + L.psi);
+  double2* gacc = reinterpret_cast<double2*>(w + L.gacc);
+  const int64_t elems = plan->state_elems;
+  if ((rc = prep<R>(plan, T, batch, angles, mats, bmat, scratch, st))) return rc;
+  JQ_CUDA(cudaMemcpyAsync(psi, state, sizeof(C) * elems * batch, cudaMemcpyDeviceToDevice, st));
+  if ((rc = seed_sv<R>(plan, T, batch, out_type, psi, ct, ct_state, lam, st))) return rc;
+  const bool want_grad = (grad_angles || grad_mats) && plan->grad_stride > 0;
+  if (want_grad) JQ_CUDA(cudaMemsetAsync(gacc, 0, 16 * static_cast<size_t>(plan->grad_stride) * batch, st));
+  const Schedule& sch = plan->adj;
+  for (size_t pi = sch.passes.size(); pi-- > 0;) {
+    const PassDesc& pd = sch.passes[pi];
+    if (pd.op_end == pd.op_begin) continue;
+    const size_t smem = tile_smem<R>(pd, 2);
+    const int64_t ntiles = (1LL << (plan->n_bits - pd.t)) * batch;
+    const int ctas = ctas_for(k_tile_adj<R>, plan->threads, smem, ntiles);
+    k_tile_adj<R><<<ctas, plan->threads, smem, st>>>(psi, lam, plan->n_bits, batch, pd, T->adj_ops, bmat,
+                                                      plan->bmat_stride, T->perm_pool, want_grad ? gacc : nullptr,
+                                                      plan->grad_stride);
+  }
+  JQ_CUDA(cudaGetLastError());
+  if (grad_init) JQ_CUDA(cudaMemcpyAsync(grad_init, lam, sizeof(C) * elems * batch, cudaMemcpyDeviceToDevice, st));
+  if ((grad_angles || grad_mats)) {
+    if ((rc = chain<R>(plan, T, batch, angles, mats, gacc, scratch, grad_angles, grad_mats, st))) return rc;
+  }
+  return JQ_OK;
+}
+
+template <typename R>
+int backward_impl(const jq_plan* plan, int batch, const double* angles, const void* mats, const void* init,
+                  int init_batched, int out_type, const double* ct, const void* ct_state, double* grad_angles,
+                  void* grad_mats, void* grad_init, void* ws, size_t ws_bytes, cudaStream_t st) {
+  using C = typename CplxT<R>::T;
+  const DeviceTables* T = nullptr;
+  int rc = device_tables(plan, &T);
+  if (rc) return rc;
+  if ((rc = set_smem_attrs<R>())) return rc;
+  WsLayout L = layout(plan, batch, 2);
+  if (ws_bytes < L.total || !ws) {
+    set_error("workspace too small: need " + std::to_string(L.total) + " bytes");
+    return JQ_ENOMEM;
+  }
+  char* w = static_cast<char*>(ws);
+  C* bmat = reinterpret_cast<C*>(w + L.bmat);
+  double2* scratch = reinterpret_cast<double2*>(w + L.scratch);
+  C* lam = reinterpret_cast<C*>(w + L.lam);
+  C* work = reinterpret_cast<C*>(w + L.work);
+  double2* gacc = reinterpret_cast<double2*>(w + L.gacc);
+  const int64_t elems = plan->state_elems;
+  const size_t sbytes = align256(sizeof(C) * elems * batch);
+  auto ckpt = [&](int64_t i) { return reinterpret_cast<C*>(w + L.ckpt + sbytes * i); };
+  auto seg = [&](int64_t i) { return reinterpret_cast<C*>(w + L.seg + sbytes * i); };
+  if ((rc = prep<R>(plan, T, batch, angles, mats, bmat, scratch, st))) return rc;
+  const bool dm = plan->mode == JQ_DENSITY;
+  const int64_t dim = 1LL << plan->n_qubits;
+  k_init<R><<<grid_for(elems * batch, 256), 256, 0, st>>>(work, elems, batch, static_cast<const C*>(init), dim,
+                                                          init_batched, dm && init ? 1 : 0);
+  JQ_CUDA(cudaGetLastError());
+  const Schedule& sch = plan->bwd;
+  const int64_t P = static_cast<int64_t>(sch.passes.size());
+  const int64_t S = L.seg_len;
+  for (int64_t p = 0; p < P; ++p) {
+    if (p % S == 0) JQ_CUDA(cudaMemcpyAsync(ckpt(p / S), work, sizeof(C) * elems * batch, cudaMemcpyDeviceToDevice, st));
+    if ((rc = run_passes<R>(plan, sch, T->bwd_ops, T, work, batch, bmat, p, p + 1, st))) return rc;
+  }
+  // seed
+  if (dm) rc = seed_dm<R>(plan, T, batch, out_type, ct, ct_state, lam, st);
+  else rc = seed_sv<R>(plan, T, batch, out_type, work, ct, ct_state, lam, st);
+  if (rc) return rc;
+  const bool want_grad = (grad_angles || grad_mats) && plan->grad_stride > 0;
+  if (want_grad) JQ_CUDA(cudaMemsetAsync(gacc, 0, 16 * static_cast<size_t>(plan->grad_stride) * batch, st));
+  for (int64_t c = L.n_ckpt - 1; c >= 0; --c) {
+    const int64_t p0 = c * S, p1 = std::min(P, p0 + S);
+    // states before passes p0..p1-1: seg[j] = state before pass p0 + j
+    JQ_CUDA(cudaMemcpyAsync(seg(0), ckpt(c), sizeof(C) * elems * batch, cudaMemcpyDeviceToDevice, st));
+    for (int64_t j = 0; j + 1 < p1 - p0; ++j) {
+      JQ_CUDA(cudaMemcpyAsync(seg(j + 1), seg(j), sizeof(C) * elems * batch, cudaMemcpyDeviceToDevice, st));
+      if ((rc = run_passes<R>(plan, sch, T->bwd_ops, T, seg(j + 1), batch, bmat, p0 + j, p0 + j + 1, st))) return rc;
+    }
+    for (int64_t p = p1 - 1; p >= p0; --p) {
+      const PassDesc& pd = sch.passes[p];
+      if (pd.op_end == pd.op_begin) continue;
+      const size_t smem = tile_smem<R>(pd, 2);
+      const int64_t ntiles = (1LL << (plan->n_bits - pd.t)) * batch;
+      const int ctas = ctas_for(k_tile_bwd<R>, plan->threads, smem, ntiles);
+      k_tile_bwd<R><<<ctas, plan->threads, smem, st>>>(seg(p - p0), lam, plan->n_bits, batch, pd, T->bwd_ops, bmat,
+                                                        plan->bmat_stride, T->perm_pool, want_grad ? gacc : nullptr,
+                                                        plan->grad_stride);
+    }
+    JQ_CUDA(cudaGetLastError());
+  }
+  if (grad_init) {
+    if (dm) {
+      if (!init) {
+        set_error("grad_init requested without an initial state");
+        return JQ_EINVAL;
+      }
+      k_grad_init_dm<R><<<grid_for(dim * batch, 256), 256, 0, st>>>(lam, static_cast<const C*>(init), init_batched,
+                                                                     static_cast<C*>(grad_init), dim, batch);
+      JQ_CUDA(cudaGetLastError());
+    } else {
+      JQ_CUDA(cudaMemcpyAsync(grad_init, lam, sizeof(C) * elems * batch, cudaMemcpyDeviceToDevice, st));
+    }
+  }
+  if (grad_angles || grad_mats) {
+    if ((rc = chain<R>(plan, T, batch, angles, mats, gacc, scratch, grad_angles, grad_mats, st))) return rc;
+  }
+  return JQ_OK;
+}
+
+}  // namespace
+}  // namespace jq
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+using namespace jq;
+
+extern "C" {
+
+int jq_plan_build(const jq_op* ops, int n_ops, const jq_obs* obs, int n_obs, int n_qubits, int mode, int dtype,
+                  const jq_tune* tune, jq_plan** out) {
+  try {
+    return build_plan(ops, n_ops, obs, n_obs, n_qubits, mode, dtype, tune, out);
+  } catch (const std::exception& e) {
+    set_error(std::string("jq_plan_build: ") + e.what());
+    return JQ_EINVAL;
+  }
+}
+
+int jq_plan_free(jq_plan* plan) {
+  if (!plan) return JQ_OK;
+  int cur = -1;
+  cudaGetDevice(&cur);
+  for (DeviceTables& t : plan->dev) {
+    if (t.device >= 0) cudaSetDevice(t.device);
+    cudaFree(t.ops); cudaFree(t.prims); cudaFree(t.blocks); cudaFree(t.fwd_ops); cudaFree(t.adj_ops);
+    cudaFree(t.bwd_ops); cudaFree(t.const_pool); cudaFree(t.perm_pool); cudaFree(t.obs_pool); cudaFree(t.obs_desc);
+  }
+  if (cur >= 0 && !plan->dev.empty()) cudaSetDevice(cur);
+  delete plan;
+  return JQ_OK;
+}
+
+int jq_plan_get_info(const jq_plan* plan, jq_plan_info* info) {
+  if (!plan || !info) { set_error("jq_plan_get_info: NULL argument"); return JQ_EINVAL; }
+  std::memset(info, 0, sizeof(*info));
+  info->n_qubits = plan->n_qubits;
+  info->n_bits = plan->n_bits;
+  info->mode = plan->mode;
+  info->dtype = plan->dtype;
+  info->n_ops = static_cast<int32_t>(plan->ops.size());
+  info->n_blocks = static_cast<int32_t>(plan->blocks.size());
+  info->n_passes_fwd = static_cast<int32_t>(plan->fwd.passes.size());
+  info->n_passes_adj = static_cast<int32_t>(plan->adj.passes.size());
+  info->n_tile_ops_fwd = static_cast<int32_t>(plan->fwd.ops.size());
+  info->tile_bits_fwd = plan->fwd.t;
+  info->tile_bits_adj = plan->adj.t;
+  info->n_angles = plan->n_angles;
+  info->n_mats = plan->n_mats;
+  info->n_obs = static_cast<int32_t>(plan->obs.size());
+  info->unitary = plan->unitary ? 1 : 0;
+  info->state_elems = plan->state_elems;
+  return JQ_OK;
+}
+
+int jq_plan_block_passes(const jq_plan* plan, int which, int32_t* block_pass, int32_t* block_wires, int n) {
+  if (!plan || !block_pass || which < 0 || which > 2) { set_error("jq_plan_block_passes: bad argument"); return JQ_EINVAL; }
+  if (n < static_cast<int>(plan->blocks.size())) { set_error("jq_plan_block_passes: array too short"); return JQ_EINVAL; }
+  const Schedule& s = which == 0 ? plan->fwd : which == 1 ? plan->adj : plan->bwd;
+  for (int b = 0; b < n; ++b) block_pass[b] = -1;
+  for (size_t p = 0; p < s.passes.size(); ++p)
+    for (int o = s.passes[p].op_begin; o < s.passes[p].op_end; ++o) block_pass[s.ops[o].block] = static_cast<int32_t>(p);
+  if (block_wires) {
+    for (size_t b = 0; b < plan->block_wires.size(); ++b)
+      for (int j = 0; j < kMaxBlockWires; ++j) block_wires[b * kMaxBlockWires + j] = plan->block_wires[b][j];
+  }
+  return JQ_OK;
+}
+
+size_t jq_workspace_bytes(const jq_plan* plan, int batch, int out_type, int with_grad) {
+  (void)out_type;
+  if (!plan || batch < 1) return 0;
+  int mode = 0;
+  if (with_grad == 1) mode = 1;       // jq_adjoint
+  else if (with_grad == 2) mode = 2;  // jq_backward
+  return layout(plan, batch, mode).total;
+}
+
+static int check_common(const jq_plan* plan, int batch, const double* angles, const void* mats) {
+  if (!plan) { set_error("NULL plan"); return JQ_EINVAL; }
+  if (batch < 1) { set_error("batch must be >= 1"); return JQ_EINVAL; }
+  if (plan->n_angles > 0 && !angles) { set_error("plan needs angles but none given"); return JQ_EINVAL; }
+  if (plan->n_mats > 0 && !mats) { set_error("plan needs matrices but none given"); return JQ_EINVAL; }
+  return JQ_OK;
+}
+
+int jq_forward(const jq_plan* plan, int batch, const double* angles, const void* mats, const void* init,
+               int init_batched, int out_type, void* state, void* out, void* workspace, size_t workspace_bytes,
+               void* stream) {
+  int rc = check_common(plan, batch, angles, mats);
+  if (rc) return rc;
+  if (!state) { set_error("jq_forward: state buffer is NULL"); return JQ_EINVAL; }
+  if (out_type != JQ_OUT_STATE && !(out_type == JQ_OUT_DENSITY && plan->mode == JQ_DENSITY) && !out &&
+      !(out_type == JQ_OUT_EXPVAL && plan->obs.empty())) {
+    set_error("jq_forward: out buffer is NULL");
+    return JQ_EINVAL;
+  }
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (plan->dtype == JQ_C64)
+    return forward_impl<float>(plan, batch, angles, mats, init, init_batched, out_type, state, out, workspace,
+                               workspace_bytes, st);
+  return forward_impl<double>(plan, batch, angles, mats, init, init_batched, out_type, state, out, workspace,
+                              workspace_bytes, st);
+}
+
+int jq_adjoint(const jq_plan* plan, int batch, const double* angles, const void* mats, const void* state,
+               int out_type, const double* ct, const void* ct_state, double* grad_angles, void* grad_mats,
+               void* grad_init, void* workspace, size_t workspace_bytes, void* stream) {
+  int rc = check_common(plan, batch, angles, mats);
+  if (rc) return rc;
+  if (!state) { set_error("jq_adjoint: state is NULL"); return JQ_EINVAL; }
+  if (out_type == JQ_OUT_EXPVAL ? (!ct && !plan->obs.empty()) : !ct_state) {
+    set_error("jq_adjoint: missing cotangent");
+    return JQ_EINVAL;
+  }
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (plan->dtype == JQ_C64)
+    return adjoint_impl<float>(plan, batch, angles, mats, state, out_type, ct, ct_state, grad_angles, grad_mats,
+                               grad_init, workspace, workspace_bytes, st);
+  return adjoint_impl<double>(plan, batch, angles, mats, state, out_type, ct, ct_state, grad_angles, grad_mats,
+                              grad_init, workspace, workspace_bytes, st);
+}
+
+int jq_backward(const jq_plan* plan, int batch, const double* angles, const void* mats, const void* init,
+                int init_batched, int out_type, const double* ct, const void* ct_state, double* grad_angles,
+                void* grad_mats, void* grad_init, void* workspace, size_t workspace_bytes, void* stream) {
+  int rc = check_common(plan, batch, angles, mats);
+  if (rc) return rc;
+  if (out_type == JQ_OUT_EXPVAL ? (!ct && !plan->obs.empty()) : !ct_state) {
+    set_error("jq_backward: missing cotangent");
+    return JQ_EINVAL;
+  }
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (plan->dtype == JQ_C64)
+    return backward_impl<float>(plan, batch, angles, mats, init, init_batched, out_type, ct, ct_state, grad_angles,
+                                grad_mats, grad_init, workspace, workspace_bytes, st);
+  return backward_impl<double>(plan, batch, angles, mats, init, init_batched, out_type, ct, ct_state, grad_angles,
+                               grad_mats, grad_init, workspace, workspace_bytes, st);
+}
+
+const char* jq_last_error(void) { return g_last_error.c_str(); }
+
+const char* jq_version(void) { return "jqsim 0.1.0 (sm_100a)"; }
+
+}  // extern "C"

@@ -1,0 +1,571 @@
+// Host planner of libjqsim: lowers a recorded tape into prims on the
+// (2n-)bit vector, fuses them into blocks and schedules the blocks into tile
+// passes.  No CUDA call is made here, so plans can be built and inspected on
+// a machine without a GPU.
+//
+// Reference behaviour restated (jaqsi/simulation.py):
+//   _fuse             :214-240  same-wire fusion rule (kept exactly, plus a cap
+//                               on the run length)
+//   _fused_structure  :202-211  structure of a fused product
+//   _compile_mixed    :348-381  gates and channels as superoperators on the
+//                               (ket, bra) axes of the density tensor
+// The pass scheduler has no reference counterpart: the reference runs one
+// XLA pass per fused entry, here one pass applies every block whose bits fit
+// in the pass's tile.
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+
+#include "jq_internal.h"
+
+namespace jq {
+
+using cd = std::complex<double>;
+
+thread_local std::string g_last_error;
+
+void set_error(const std::string& msg) { g_last_error = msg; }
+
+namespace {
+
+struct HostPrim {
+  int op = -1;
+  int form = PF_U;
+  std::vector<int> wires;      // wires on the bit vector (n or 2n wires)
+  Structure st;
+  std::vector<cd> cmat;        // PF_CONST: full matrix
+};
+
+struct HostBlock {
+  std::vector<int> wires;
+  Structure st;
+  std::vector<int> prims;
+};
+
+std::vector<cd> read_matrix(const double* p, int dim) {
+  std::vector<cd> m(static_cast<size_t>(dim) * dim);
+  for (size_t i = 0; i < m.size(); ++i) m[i] = cd(p[2 * i], p[2 * i + 1]);
+  return m;
+}
+
+std::vector<cd> kron(const std::vector<cd>& a, int da, const std::vector<cd>& b, int db) {
+  int d = da * db;
+  std::vector<cd> r(static_cast<size_t>(d) * d);
+  for (int i = 0; i < da; ++i)
+    for (int j = 0; j < da; ++j)
+      for (int p = 0; p < db; ++p)
+        for (int q = 0; q < db; ++q)
+          r[static_cast<size_t>(i * db + p) * d + (j * db + q)] = a[i * da + j] * b[p * db + q];
+  return r;
+}
+
+std::vector<cd> conj_of(const std::vector<cd>& a) {
+  std::vector<cd> r(a.size());
+  for (size_t i = 0; i < a.size(); ++i) r[i] = std::conj(a[i]);
+  return r;
+}
+
+// Structure read off the values of a constant matrix: diagonal, permutation
+// (exact 0/1 entries) and leading controls (identity on every index whose
+// control bits are not all one).
+Structure detect_structure(const std::vector<cd>& m, int k) {
+  Structure st;
+  int d = 1 << k;
+  bool diag = true, perm = true;
+  std::vector<int32_t> p(d, -1);
+  for (int i = 0; i < d; ++i) {
+    int ones = 0;
+    for (int j = 0; j < d; ++j) {
+      cd v = m[static_cast<size_t>(i) * d + j];
+      if (i != j && v != cd(0, 0)) diag = false;
+      if (v == cd(1, 0)) {
+        ++ones;
+        p[i] = j;
+      } else if (v != cd(0, 0)) {
+        perm = false;
+      }
+    }
+    if (ones != 1) perm = false;
+  }
+  if (perm) {
+    std::vector<int> seen(d, 0);
+    for (int i = 0; i < d; ++i) {
+      if (p[i] < 0 || seen[p[i]]) { perm = false; break; }
+      seen[p[i]] = 1;
+    }
+  }
+  st.diagonal = diag;
+  if (perm) st.perm = p;
+  // controls: largest c such that m = I (+) inner with inner 2^(k-c) square
+  for (int c = k - 1; c >= 1; --c) {
+    int inner = 1 << (k - c);
+    int base = d - inner;
+    bool ok = true;
+    for (int i = 0; i < d && ok; ++i)
+      for (int j = 0; j < d && ok; ++j) {
+        if (i >= base && j >= base) continue;
+        cd want = (i == j) ? cd(1, 0) : cd(0, 0);
+        if (m[static_cast<size_t>(i) * d + j] != want) ok = false;
+      }
+    if (ok) { st.controls = c; break; }
+  }
+  return st;
+}
+
+// GateStructure of a product right @ left on identical wires
+// (jaqsi/simulation.py:202-211).
+Structure fused_structure(const Structure& left, const Structure& right) {
+  Structure st;
+  if (!left.perm.empty() && !right.perm.empty()) {
+    st.perm.resize(right.perm.size());
+    for (size_t i = 0; i < right.perm.size(); ++i) st.perm[i] = left.perm[right.perm[i]];
+  }
+  st.diagonal = left.diagonal && right.diagonal;
+  st.controls = std::min(left.controls, right.controls);
+  return st;
+}
+
+int popcount64(uint64_t x) { return __builtin_popcountll(x); }
+
+bool validate_perm(const std::vector<int32_t>& p, int d) {
+  if (static_cast<int>(p.size()) != d) return false;
+  std::vector<int> seen(d, 0);
+  for (int v : p) {
+    if (v < 0 || v >= d || seen[v]) return false;
+    seen[v] = 1;
+  }
+  return true;
+}
+
+// Greedy tile-pass scheduler.  Walks the blocks in program order; a block
+// joins the current pass when none of its bits is blocked and the pass's bit
+// set stays within t bits; otherwise its bits become blocked for the rest of
+// the pass (a later block on those bits must follow it).  Members of a pass
+// therefore never depend on a deferred block, and program order is kept.
+Schedule schedule(const std::vector<HostBlock>& blocks, const std::vector<DevBlock>& dblocks,
+                  int nb, int t_max, int c_seed, bool one_per_pass) {
+  Schedule s;
+  s.t = t_max;
+  int nblk = static_cast<int>(blocks.size());
+  std::vector<char> done(nblk, 0);
+  int cursor = 0;
+  const uint64_t all_bits = (nb >= 64) ? ~0ULL : ((1ULL << nb) - 1);
+  auto block_bits = [&](int b) {
+    uint64_t m = 0;
+    for (int w : blocks[b].wires) m |= 1ULL << (nb - 1 - w);
+    return m;
+  };
+  while (cursor < nblk) {
+    uint64_t S = (c_seed >= 64) ? ~0ULL : ((1ULL << c_seed) - 1);
+    uint64_t blocked = 0;
+    std::vector<int> members;
+    for (int b = cursor; b < nblk; ++b) {
+      if (done[b]) continue;
+      uint64_t bb = block_bits(b);
+      if (bb & blocked) { blocked |= bb; continue; }
+      if (popcount64(S | bb) <= t_max && !(one_per_pass && !members.empty())) {
+        S |= bb;
+        members.push_back(b);
+        done[b] = 1;
+      } else {
+        blocked |= bb;
+      }
+      if ((blocked | 0) == all_bits) break;
+    }
+    while (cursor < nblk && done[cursor]) ++cursor;
+    PassDesc pd;
+    std::memset(&pd, 0, sizeof(pd));
+    int t = 0;
+    for (int bit = 0; bit < nb; ++bit)
+      if (S >> bit & 1ULL) pd.bits[t++] = static_cast<int8_t>(bit);
+    pd.t = t;
+    pd.tile_mask = S;
+    int c = 0;
+    while (c < t && pd.bits[c] == c) ++c;
+    pd.c = c;
+    pd.op_begin = static_cast<int32_t>(s.ops.size());
+    int rank[64];
+    for (int i = 0; i < 64; ++i) rank[i] = -1;
+    for (int i = 0; i < t; ++i) rank[pd.bits[i]] = i;
+    for (int b : members) {
+      const DevBlock& db = dblocks[b];
+      TileOp op;
+      std::memset(&op, 0, sizeof(op));
+      op.block = b;
+      op.kind = db.kind;
+      op.kt = db.k - db.n_ctrl;
+      op.nfix = db.k;
+      op.ctrl_mask = 0;
+      int pos[kMaxBlockWires];
+      for (int i = 0; i < db.k; ++i) {
+        int bit = nb - 1 - blocks[b].wires[i];
+        pos[i] = rank[bit];
+        if (i < db.n_ctrl) op.ctrl_mask |= 1u << pos[i];
+        else op.tb[i - db.n_ctrl] = static_cast<int8_t>(pos[i]);
+      }
+      std::sort(pos, pos + db.k);
+      for (int i = 0; i < db.k; ++i) op.fix[i] = static_cast<int8_t>(pos[i]);
+      op.mat_off = db.mat_off;
+      op.perm_off = db.perm_off;
+      op.grad_off = db.grad_off;
+      s.ops.push_back(op);
+    }
+    pd.op_end = static_cast<int32_t>(s.ops.size());
+    s.passes.push_back(pd);
+  }
+  return s;
+}
+
+int default_tile_bits(int nb, int dtype, int maxk, int c_seed, bool adjoint) {
+  int t = (dtype == JQ_C64) ? 14 : 13;
+  if (adjoint) t -= 1;
+  // keep at least ~256 tiles per state when the state is large enough
+  int floor_t = std::max(10, maxk + c_seed);
+  if (nb - 8 < t) t = std::max(nb - 8, floor_t);
+  if (t > nb) t = nb;
+  return t;
+}
+
+}  // namespace
+
+int build_plan(const jq_op* ops, int n_ops, const jq_obs* obs, int n_obs, int n_qubits, int mode,
+               int dtype, const jq_tune* tune, jq_plan** out) {
+  if (!out) { set_error("jq_plan_build: out is NULL"); return JQ_EINVAL; }
+  *out = nullptr;
+  if (mode != JQ_STATEVECTOR && mode != JQ_DENSITY) { set_error("jq_plan_build: bad mode"); return JQ_EINVAL; }
+  if (dtype != JQ_C64 && dtype != JQ_C128) { set_error("jq_plan_build: bad dtype"); return JQ_EINVAL; }
+  if (n_qubits < 1 || n_qubits > JQ_MAX_QUBITS || (mode == JQ_DENSITY && n_qubits > JQ_MAX_QUBITS / 2)) {
+    set_error("jq_plan_build: n_qubits out of range (" + std::to_string(n_qubits) + ")");
+    return JQ_EINVAL;
+  }
+  if (n_ops < 0 || (n_ops > 0 && !ops) || n_obs < 0 || (n_obs > 0 && !obs)) {
+    set_error("jq_plan_build: bad op / observable arrays");
+    return JQ_EINVAL;
+  }
+  jq_plan* plan = new (std::nothrow) jq_plan();
+  if (!plan) { set_error("jq_plan_build: out of host memory"); return JQ_ENOMEM; }
+  plan->n_qubits = n_qubits;
+  plan->mode = mode;
+  plan->dtype = dtype;
+  const int n = n_qubits;
+  const int nb = (mode == JQ_DENSITY) ? 2 * n : n;
+  plan->n_bits = nb;
+  plan->state_elems = 1LL << nb;
+
+  std::vector<HostPrim> prims;
+  auto fail = [&](const std::string& msg) {
+    set_error(msg);
+    delete plan;
+    return JQ_EINVAL;
+  };
+
+  // ---- ops -> DevOp + prims ------------------------------------------------
+  for (int i = 0; i < n_ops; ++i) {
+    const jq_op& o = ops[i];
+    int k = o.n_wires;
+    if (k < 1 || k > JQ_MAX_OP_WIRES) return fail("op " + std::to_string(i) + ": wire count out of range");
+    for (int a = 0; a < k; ++a) {
+      if (o.wires[a] < 0 || o.wires[a] >= n)
+        return fail("op " + std::to_string(i) + ": wire " + std::to_string(o.wires[a]) + " outside 0.." + std::to_string(n - 1));
+      for (int b = 0; b < a; ++b)
+        if (o.wires[a] == o.wires[b]) return fail("op " + std::to_string(i) + ": duplicate wires");
+    }
+    DevOp d;
+    std::memset(&d, 0, sizeof(d));
+    d.kind = o.kind;
+    d.k = k;
+    d.n_ctrl = o.n_controls;
+    d.angle_slot = o.angle_slot;
+    d.mat_slot = o.mat_slot;
+    d.mat_is_diag = o.mat_is_diag;
+    d.px = o.pauli_x;
+    d.pz = o.pauli_z;
+    d.grad = o.grad;
+    switch (o.kind) {
+      case JQ_K_CONST: case JQ_K_MATRIX: case JQ_K_CHANNEL: d.n_angles = 0; break;
+      case JQ_K_RX: case JQ_K_RY: case JQ_K_RZ: case JQ_K_CPHASE: case JQ_K_PAULIROT: d.n_angles = 1; break;
+      case JQ_K_ROT: d.n_angles = 3; break;
+      default: return fail("op " + std::to_string(i) + ": unknown kind " + std::to_string(o.kind));
+    }
+    if ((o.kind == JQ_K_RX || o.kind == JQ_K_RY || o.kind == JQ_K_RZ || o.kind == JQ_K_ROT) && k != 1)
+      return fail("op " + std::to_string(i) + ": single-qubit rotation on " + std::to_string(k) + " wires");
+    if (o.kind == JQ_K_PAULIROT && (o.n_controls < 0 || o.n_controls >= k))
+      return fail("op " + std::to_string(i) + ": bad control count");
+    if (d.n_angles > 0) {
+      if (o.angle_slot < 0) return fail("op " + std::to_string(i) + ": negative angle slot");
+      plan->n_angles = std::max(plan->n_angles, o.angle_slot + d.n_angles);
+    }
+    if (o.kind == JQ_K_MATRIX) {
+      if (o.mat_slot < 0) return fail("op " + std::to_string(i) + ": negative matrix slot");
+      int len = o.mat_is_diag ? (1 << k) : (1 << (2 * k));
+      plan->n_mats = std::max(plan->n_mats, o.mat_slot + len);
+    }
+    if (!o.unitary) plan->unitary = false;
+    if (o.kind == JQ_K_CHANNEL) plan->unitary = false;
+    if (o.grad && (d.n_angles > 0 || o.kind == JQ_K_MATRIX)) plan->any_grad = true;
+    plan->ops.push_back(d);
+
+    // declared structure of the op
+    Structure st;
+    int dim = 1 << k;
+    if (o.has_perm) {
+      st.perm.assign(o.perm, o.perm + dim);
+      if (!validate_perm(st.perm, dim)) return fail("op " + std::to_string(i) + ": invalid permutation");
+    }
+    st.diagonal = o.diagonal != 0;
+    st.controls = std::max(0, std::min(o.n_controls, k - 1));
+    if (o.kind == JQ_K_MATRIX && o.mat_is_diag) { st.diagonal = true; st.perm.clear(); }
+
+    std::vector<int> ket(o.wires, o.wires + k);
+    std::vector<int> bra(k);
+    for (int a = 0; a < k; ++a) bra[a] = o.wires[a] + n;
+
+    if (o.kind == JQ_K_CHANNEL) {
+      if (mode != JQ_DENSITY)
+        return fail("op " + std::to_string(i) + ": a noise channel cannot be applied to a pure statevector");
+      if (2 * k > kMaxBlockWires) return fail("op " + std::to_string(i) + ": channel on more than 3 wires");
+      if (o.n_kraus < 1 || !o.const_mat) return fail("op " + std::to_string(i) + ": channel without Kraus matrices");
+      int dd = dim * dim;
+      std::vector<cd> sup(static_cast<size_t>(dd) * dd, cd(0, 0));
+      for (int q = 0; q < o.n_kraus; ++q) {
+        std::vector<cd> K = read_matrix(o.const_mat + 2 * static_cast<size_t>(q) * dim * dim, dim);
+        std::vector<cd> kk = kron(K, dim, conj_of(K), dim);
+        for (size_t e = 0; e < sup.size(); ++e) sup[e] += kk[e];
+      }
+      HostPrim p;
+      p.op = i;
+      p.form = PF_CONST;
+      p.wires = ket;
+      p.wires.insert(p.wires.end(), bra.begin(), bra.end());
+      p.st = detect_structure(sup, 2 * k);
+      p.cmat = std::move(sup);
+      prims.push_back(std::move(p));
+      continue;
+    }
+    if (o.kind == JQ_K_CONST && !o.const_mat) return fail("op " + std::to_string(i) + ": constant op without matrix");
+
+    if (mode == JQ_STATEVECTOR) {
+      HostPrim p;
+      p.op = i;
+      p.wires = ket;
+      if (o.kind == JQ_K_CONST) {
+        p.form = PF_CONST;
+        p.cmat = read_matrix(o.const_mat, dim);
+        p.st = detect_structure(p.cmat, k);
+      } else {
+        p.form = PF_U;
+        p.st = st;
+      }
+      prims.push_back(std::move(p));
+    } else if (k == 1) {
+      // 1-qubit gate on a density matrix: superoperator kron(U, conj U) on the
+      // (ket, bra) wires, so it fuses with the channels on the same wire.
+      HostPrim p;
+      p.op = i;
+      p.wires = {ket[0], bra[0]};
+      if (o.kind == JQ_K_CONST) {
+        std::vector<cd> U = read_matrix(o.const_mat, 2);
+        p.form = PF_CONST;
+        p.cmat = kron(U, 2, conj_of(U), 2);
+        p.st = detect_structure(p.cmat, 2);
+      } else {
+        p.form = PF_KRON;
+        p.st.diagonal = st.diagonal;
+        p.st.controls = 0;
+        if (!st.perm.empty()) {
+          p.st.perm.resize(4);
+          for (int a = 0; a < 2; ++a)
+            for (int b = 0; b < 2; ++b) p.st.perm[a * 2 + b] = st.perm[a] * 2 + st.perm[b];
+        }
+      }
+      prims.push_back(std::move(p));
+    } else {
+      // wider gate on a density matrix: U on the ket wires, conj(U) on the bra
+      // wires, each keeping its structure.
+      HostPrim pk, pb;
+      pk.op = pb.op = i;
+      pk.wires = ket;
+      pb.wires = bra;
+      if (o.kind == JQ_K_CONST) {
+        std::vector<cd> U = read_matrix(o.const_mat, dim);
+        pk.form = pb.form = PF_CONST;
+        pk.cmat = U;
+        pb.cmat = conj_of(U);
+        pk.st = detect_structure(pk.cmat, k);
+        pb.st = detect_structure(pb.cmat, k);
+      } else {
+        pk.form = PF_U;
+        pb.form = PF_CONJ;
+        pk.st = pb.st = st;
+      }
+      prims.push_back(std::move(pk));
+      prims.push_back(std::move(pb));
+    }
+  }
+
+  // ---- same-wire fusion (jaqsi _fuse, simulation.py:214-240) ----------------
+  const bool no_fuse = tune && tune->no_fuse;
+  std::vector<HostBlock> blocks;
+  {
+    std::vector<int> last(nb, -1);
+    for (int pi = 0; pi < static_cast<int>(prims.size()); ++pi) {
+      const HostPrim& p = prims[pi];
+      int bi = last[p.wires[0]];
+      bool merge = !no_fuse && bi >= 0 && blocks[bi].wires == p.wires &&
+                   static_cast<int>(blocks[bi].prims.size()) < kMaxFusePrims;
+      if (merge)
+        for (int w : p.wires)
+          if (last[w] != bi) { merge = false; break; }
+      if (merge) {
+        blocks[bi].st = fused_structure(blocks[bi].st, p.st);
+        blocks[bi].prims.push_back(pi);
+        continue;
+      }
+      HostBlock b;
+      b.wires = p.wires;
+      b.st = p.st;
+      b.prims.push_back(pi);
+      blocks.push_back(std::move(b));
+      for (int w : p.wires) last[w] = static_cast<int>(blocks.size()) - 1;
+    }
+  }
+
+  // ---- device prims / blocks -----------------------------------------------
+  int maxk = 1;
+  for (const HostBlock& b : blocks) maxk = std::max(maxk, static_cast<int>(b.wires.size()));
+  std::vector<int> prim_order;
+  int64_t bmat = 0, grad = 0, scratch = 0;
+  for (const HostBlock& hb : blocks) {
+    DevBlock db;
+    std::memset(&db, 0, sizeof(db));
+    int k = static_cast<int>(hb.wires.size());
+    int dim = 1 << k;
+    db.k = k;
+    db.prim_begin = static_cast<int32_t>(plan->prims.size());
+    bool needs_grad = false;
+    for (int pi : hb.prims) {
+      const HostPrim& p = prims[pi];
+      DevPrim dp;
+      dp.op = p.op;
+      dp.form = p.form;
+      dp.k = static_cast<int32_t>(p.wires.size());
+      dp.const_off = -1;
+      if (p.form == PF_CONST) {
+        dp.const_off = static_cast<int32_t>(plan->const_pool.size() / 2);
+        for (const cd& v : p.cmat) {
+          plan->const_pool.push_back(v.real());
+          plan->const_pool.push_back(v.imag());
+        }
+      } else if (p.op >= 0) {
+        const DevOp& o = plan->ops[p.op];
+        if (o.grad && (o.n_angles > 0 || o.kind == JQ_K_MATRIX)) needs_grad = true;
+      }
+      plan->prims.push_back(dp);
+    }
+    db.prim_end = static_cast<int32_t>(plan->prims.size());
+    Structure st = hb.st;
+    int c = std::max(0, std::min(st.controls, k - 1));
+    if (!st.perm.empty()) {
+      // inner permutation of the controlled part
+      int d = 1 << (k - c), base = dim - d;
+      bool ok = true;
+      for (int i = 0; i < base && ok; ++i) ok = st.perm[i] == i;
+      for (int i = 0; i < d && ok; ++i) ok = st.perm[base + i] >= base;
+      if (!ok) { c = 0; d = dim; base = 0; }
+      db.kind = BK_PERM;
+      db.n_ctrl = c;
+      db.d = d;
+      db.perm_off = static_cast<int32_t>(plan->perm_pool.size());
+      for (int i = 0; i < d; ++i) plan->perm_pool.push_back(st.perm[base + i] - base);
+      db.mat_off = -1;
+      db.grad_off = -1;
+    } else {
+      db.kind = st.diagonal ? BK_DIAG : BK_DENSE;
+      db.n_ctrl = c;
+      db.d = 1 << (k - c);
+      db.perm_off = -1;
+      db.mat_off = static_cast<int32_t>(bmat);
+      bmat += (db.kind == BK_DIAG) ? db.d : static_cast<int64_t>(db.d) * db.d;
+      if (needs_grad) {
+        db.grad_off = static_cast<int32_t>(grad);
+        grad += (db.kind == BK_DIAG) ? db.d : static_cast<int64_t>(db.d) * db.d;
+      } else {
+        db.grad_off = -1;
+      }
+    }
+    if (k > 2) {
+      db.scratch_off = static_cast<int32_t>(scratch);
+      scratch += 8LL * dim * dim;
+    } else {
+      db.scratch_off = -1;
+    }
+    plan->blocks.push_back(db);
+    std::array<int32_t, kMaxBlockWires> bw;
+    bw.fill(-1);
+    for (int i = 0; i < k; ++i) bw[i] = hb.wires[i];
+    plan->block_wires.push_back(bw);
+  }
+  plan->bmat_stride = bmat;
+  plan->grad_stride = grad;
+  plan->scratch_stride = scratch;
+
+  // ---- schedules ---------------------------------------------------------------
+  const int c_seed = std::min(nb, dtype == JQ_C64 ? 4 : 3);
+  int tf = (tune && tune->tile_bits > 0) ? tune->tile_bits : default_tile_bits(nb, dtype, maxk, c_seed, false);
+  int ta = (tune && tune->tile_bits_adj > 0) ? tune->tile_bits_adj : default_tile_bits(nb, dtype, maxk, c_seed, true);
+  tf = std::min(std::min(tf, nb), kMaxTileBits);
+  ta = std::min(std::min(ta, nb), kMaxTileBits);
+  if (tf < std::min(nb, maxk + c_seed) || ta < std::min(nb, maxk + c_seed)) {
+    return fail("jq_plan_build: tile too small for a " + std::to_string(maxk) + "-wire block");
+  }
+  int max_t = (dtype == JQ_C64) ? 14 : 13;
+  if (tf > max_t || ta > max_t - 1) return fail("jq_plan_build: tile_bits too large for shared memory");
+  plan->fwd = schedule(blocks, plan->blocks, nb, tf, c_seed, no_fuse);
+  plan->adj = schedule(blocks, plan->blocks, nb, ta, c_seed, no_fuse);
+  plan->bwd = schedule(blocks, plan->blocks, nb, ta, c_seed, true);
+  plan->threads = (tune && tune->threads > 0) ? tune->threads : 512;
+  if (plan->threads % 32 || plan->threads < 64 || plan->threads > 1024)
+    return fail("jq_plan_build: threads must be a multiple of 32 in 64..1024");
+  plan->ckpt_stride = (tune && tune->ckpt_stride > 0) ? tune->ckpt_stride : 0;
+
+  // ---- observables -----------------------------------------------------------------
+  for (int i = 0; i < n_obs; ++i) {
+    const jq_obs& o = obs[i];
+    DevObs d;
+    std::memset(&d, 0, sizeof(d));
+    d.kind = o.kind;
+    d.k = o.n_wires;
+    if (o.kind == JQ_OBS_PAULI) {
+      uint64_t lim = (n >= 64) ? ~0ULL : ((1ULL << n) - 1);
+      if ((o.x_mask | o.z_mask) & ~lim) return fail("observable " + std::to_string(i) + ": Pauli mask outside the register");
+      d.x_mask = o.x_mask;
+      d.z_mask = o.z_mask;
+      d.n_y = o.n_y;
+      d.coeff = o.coeff;
+    } else if (o.kind == JQ_OBS_DENSE) {
+      int k = o.n_wires;
+      if (k < 1 || k > JQ_MAX_OP_WIRES || !o.mat) return fail("observable " + std::to_string(i) + ": bad dense observable");
+      for (int a = 0; a < k; ++a) {
+        if (o.wires[a] < 0 || o.wires[a] >= n) return fail("observable " + std::to_string(i) + ": wire out of range");
+        for (int b = 0; b < a; ++b)
+          if (o.wires[a] == o.wires[b]) return fail("observable " + std::to_string(i) + ": duplicate wires");
+        d.bits[a] = static_cast<int8_t>(n - 1 - o.wires[a]);
+      }
+      d.mat_off = static_cast<int32_t>(plan->obs_pool.size() / 2);
+      int dim = 1 << k;
+      for (int e = 0; e < 2 * dim * dim; ++e) plan->obs_pool.push_back(o.mat[e]);
+      d.coeff = 1.0;
+    } else {
+      return fail("observable " + std::to_string(i) + ": unknown kind");
+    }
+    plan->obs.push_back(d);
+  }
+  *out = plan;
+  return JQ_OK;
+}
+
+}  // namespace jq

@@ -1,0 +1,623 @@
+"""Simulation layer: the drop-in for jaqsi/simulation.py on one B200.
+
+A recorded tape is lowered to ``jq_op`` descriptors, compiled once per
+structure into a ``jq_plan`` (cached like the reference's jit cache,
+jaqsi/script.py:695-725) and executed by libjqsim through its C ABI.  Angles
+and per-call matrices are gathered into one device tensor each, so gradients
+flow back to the circuit's arguments through a single
+``torch.autograd.Function`` whose backward is the GPU adjoint
+(unitary statevector plans) or the checkpointed reverse pass (everything else).
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+import threading
+from collections import OrderedDict
+from typing import Dict, List, Optional, Sequence, Tuple
+
+import numpy as np
+import torch
+
+from jaqsi_b200 import _lib as L
+from jaqsi_b200.gateset import Barrier, Id, PauliX, PauliY, PauliZ
+from jaqsi_b200.noise import KrausChannel
+from jaqsi_b200.operations import Operation, cdtype, rdtype
+
+_TYPES = ("state", "probs", "expval", "density")
+_OUT = {"state": L.JQ_OUT_STATE, "probs": L.JQ_OUT_PROBS, "expval": L.JQ_OUT_EXPVAL, "density": L.JQ_OUT_DENSITY}
+
+
+def infer_n_qubits(ops: List[Operation], obs: List[Operation]) -> int:
+    """``max(wire) + 1`` over ops and observables (jaqsi/simulation.py:32-46)."""
+    wires = set()
+    for op in list(ops) + list(obs):
+        wires.update(op.wires)
+    return max(wires) + 1 if wires else 1
+
+
+def has_noise(tape: List[Operation]) -> bool:
+    """Whether the tape holds a Kraus channel (jaqsi/simulation.py:49-62)."""
+    return any(isinstance(op, KrausChannel) for op in tape)
+
+
+def _device() -> torch.device:
+    if not torch.cuda.is_available():
+        raise RuntimeError(
+            "jaqsi_b200 executes circuits on a CUDA GPU (sm_100a) only; no CUDA device is available"
+        )
+    return torch.device("cuda", torch.cuda.current_device())
+
+
+# ---------------------------------------------------------------------------
+# observables
+# ---------------------------------------------------------------------------
+_PAULI_WORD_OF = {PauliX: "X", PauliY: "Y", PauliZ: "Z"}
+
+
+def _concrete_matrix(ob: Operation) -> np.ndarray:
+    m = ob._matrix
+    if isinstance(m, torch.Tensor):
+        m = m.detach().cpu().numpy()
+    return np.asarray(m, dtype=np.complex128)
+
+
+def _detect_pauli(m: np.ndarray):
+    """(word masks over matrix bits, n_y, real coefficient) if *m* is a real
+    multiple of a Pauli word, else None."""
+    d = m.shape[0]
+    k = d.bit_length() - 1
+    nz = np.nonzero(np.abs(m[:, 0]) > 0)[0]
+    if len(nz) != 1:
+        return None
+    x = int(nz[0])
+    z = 0
+    base = m[x, 0]
+    for b in range(k):
+        c = 1 << b
+        v = m[c ^ x, c]
+        if abs(v - base) < 1e-14 * max(1.0, abs(base)):
+            continue
+        if abs(v + base) < 1e-14 * max(1.0, abs(base)):
+            z |= c
+        else:
+            return None
+    ny = bin(x & z).count("1")
+    ph = [1, 1j, -1, -1j][ny % 4]
+    coeff = base / ph
+    if abs(coeff.imag) > 1e-14 * max(1.0, abs(coeff)):
+        return None
+    coeff = float(coeff.real)
+    ref = np.zeros_like(m)
+    for c in range(d):
+        sign = -1.0 if bin(c & z).count("1") % 2 else 1.0
+        ref[c ^ x, c] = coeff * ph * sign
+    if not np.allclose(ref, m, atol=1e-14, rtol=0):
+        return None
+    return x, z, ny, coeff
+
+
+def _lower_obs(obs: Sequence[Operation], n: int):
+    """jq_obs records (plus keep-alive buffers) and a cache key."""
+    specs = []
+    for ob in obs:
+        wires = list(ob.wires)
+        for w in wires:
+            if w < 0 or w >= n:
+                raise ValueError(f"observable wire {w} outside 0..{n - 1}")
+        word = getattr(ob, "_pauli_label", None)
+        coeff = 1.0
+        if word is None and type(ob) in _PAULI_WORD_OF:
+            word = _PAULI_WORD_OF[type(ob)]
+        if word is None and isinstance(ob, Id):
+            word = "I" * len(wires)
+        if word is not None:
+            x = z = 0
+            ny = 0
+            for i, ch in enumerate(word):
+                bit = 1 << (n - 1 - wires[i])
+                if ch in "XY":
+                    x |= bit
+                if ch in "ZY":
+                    z |= bit
+                ny += ch == "Y"
+            specs.append(("P", x, z, ny, coeff, None, wires))
+            continue
+        m = _concrete_matrix(ob)
+        det = _detect_pauli(m)
+        if det is not None:
+            xl, zl, ny, coeff = det
+            k = len(wires)
+            x = z = 0
+            for i, w in enumerate(wires):
+                pos = 1 << (k - 1 - i)
+                if xl & pos:
+                    x |= 1 << (n - 1 - w)
+                if zl & pos:
+                    z |= 1 << (n - 1 - w)
+            specs.append(("P", x, z, ny, coeff, None, wires))
+        else:
+            if len(wires) > L.JQ_MAX_OP_WIRES:
+                raise ValueError(f"observables on more than {L.JQ_MAX_OP_WIRES} wires are not supported")
+            specs.append(("D", 0, 0, 0, 1.0, np.ascontiguousarray(m), wires))
+    key = tuple(
+        (s[0], s[1], s[2], s[3], s[4], tuple(s[6])) if s[0] == "P" else ("D", tuple(s[6]), s[5].tobytes())
+        for s in specs
+    )
+    return specs, key
+
+
+def _build_obs_array(specs):
+    arr = (L.JqObs * max(1, len(specs)))()
+    keep = []
+    for i, (kind, x, z, ny, coeff, mat, wires) in enumerate(specs):
+        o = arr[i]
+        o.kind = L.JQ_OBS_PAULI if kind == "P" else L.JQ_OBS_DENSE
+        o.n_wires = len(wires)
+        for j, w in enumerate(wires[: L.JQ_MAX_OP_WIRES]):
+            o.wires[j] = w
+        o.x_mask, o.z_mask, o.n_y, o.coeff = x, z, ny, coeff
+        if mat is not None:
+            buf = np.ascontiguousarray(mat.astype(np.complex128)).view(np.float64)
+            keep.append(buf)
+            o.mat = buf.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    return arr, keep
+
+
+# ---------------------------------------------------------------------------
+# tape lowering
+# ---------------------------------------------------------------------------
+class Lowered:
+    """Static structure of a tape (plan key + jq_op fields) and its per-call
+    values (angles and matrices)."""
+
+    __slots__ = ("key", "statics", "angles", "mats", "unitary")
+
+    def __init__(self):
+        self.key = None
+        self.statics = []
+        self.angles: list = []
+        self.mats: list = []
+        self.unitary = True
+
+
+def _is_tensor(v) -> bool:
+    return isinstance(v, torch.Tensor)
+
+
+def lower_tape(tape: Sequence[Operation], n_qubits: int) -> Lowered:
+    """Lower recorded ops to plan statics and per-call values."""
+    lw = Lowered()
+    keys = []
+    n_ang = 0
+    n_mat = 0
+    for op in tape:
+        if isinstance(op, Barrier):
+            continue
+        wires = tuple(op.wires)
+        for w in wires:
+            if w < 0 or w >= n_qubits:
+                raise ValueError(f"{op.name}: wire {w} outside 0..{n_qubits - 1}")
+        if len(wires) > L.JQ_MAX_OP_WIRES:
+            raise ValueError(f"{op.name}: gates on more than {L.JQ_MAX_OP_WIRES} wires are not supported")
+        kind, angles, payload = op._jq_lower()
+        st = op._structure
+        unitary = bool(op.is_unitary)
+        grad = 0
+        angle_slot = -1
+        mat_slot = -1
+        mat_is_diag = 0
+        if angles:
+            angle_slot = n_ang
+            n_ang += len(angles)
+            lw.angles.extend(angles)
+            grad = int(any(_is_tensor(a) for a in angles))
+        if kind == L.JQ_K_MATRIX:
+            mat_slot = n_mat
+            t = payload
+            mat_is_diag = int(t.dim() == 1)
+            n_mat += t.numel()
+            lw.mats.append(t)
+            grad = 1
+        skey = op._jq_static_key()
+        px = getattr(op, "_px", 0)
+        pz = getattr(op, "_pz", 0)
+        nctrl = getattr(op, "n_controls", 0) if kind == L.JQ_K_PAULIROT else st.controls
+        keys.append((skey, wires, st, grad, unitary, mat_is_diag))
+        lw.statics.append((kind, wires, st, angle_slot, mat_slot, mat_is_diag, px, pz, nctrl, payload, grad, unitary))
+        if not unitary:
+            lw.unitary = False
+    lw.key = tuple(keys)
+    return lw
+
+
+def _build_op_array(statics):
+    arr = (L.JqOp * max(1, len(statics)))()
+    keep = []
+    for i, (kind, wires, st, angle_slot, mat_slot, mat_is_diag, px, pz, nctrl, payload, grad, unitary) in enumerate(statics):
+        o = arr[i]
+        o.kind = kind
+        o.n_wires = len(wires)
+        for j, w in enumerate(wires):
+            o.wires[j] = w
+        o.n_controls = int(nctrl)
+        o.diagonal = int(bool(st.diagonal))
+        if st.permutation:
+            o.has_perm = 1
+            for j, p in enumerate(st.permutation):
+                o.perm[j] = int(p)
+        o.angle_slot = angle_slot
+        o.mat_slot = mat_slot
+        o.mat_is_diag = mat_is_diag
+        o.pauli_x, o.pauli_z = int(px), int(pz)
+        o.grad = grad
+        o.unitary = int(unitary)
+        if kind == L.JQ_K_CONST:
+            buf = np.ascontiguousarray(payload, dtype=np.complex128).view(np.float64)
+            keep.append(buf)
+            o.const_mat = buf.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+        elif kind == L.JQ_K_CHANNEL:
+            buf = np.ascontiguousarray(np.stack(payload), dtype=np.complex128).view(np.float64)
+            keep.append(buf)
+            o.n_kraus = len(payload)
+            o.const_mat = buf.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    return arr, keep
+
+
+# ---------------------------------------------------------------------------
+# plans
+# ---------------------------------------------------------------------------
+class Plan:
+    """An immutable libjqsim execution plan (freed with the object)."""
+
+    def __init__(self, statics, obs_specs, n_qubits: int, mode: int, dtype: torch.dtype, tune: Optional[dict] = None):
+        ops, keep_ops = _build_op_array(statics)
+        obs_arr, keep_obs = _build_obs_array(obs_specs)
+        t = L.JqTune()
+        for k, v in (tune or {}).items():
+            setattr(t, k, int(v))
+        handle = ctypes.c_void_p()
+        lib = L.lib()
+        L.check(
+            lib.jq_plan_build(
+                ops, len(statics), obs_arr, len(obs_specs), n_qubits, mode,
+                L.JQ_C64 if dtype == torch.complex64 else L.JQ_C128, ctypes.byref(t), ctypes.byref(handle),
+            )
+        )
+        self._lib = lib
+        self.handle = handle
+        info = L.JqPlanInfo()
+        L.check(lib.jq_plan_get_info(handle, ctypes.byref(info)))
+        self.info = info.as_dict()
+        self.n_qubits = n_qubits
+        self.mode = mode
+        self.cdtype = dtype
+        self.rdtype = rdtype(dtype)
+        self.n_obs = len(obs_specs)
+        self.state_elems = info.state_elems
+        self.n_angles = info.n_angles
+        self.n_mats = info.n_mats
+        self.unitary = bool(info.unitary)
+        del keep_ops, keep_obs  # the plan copied everything it needs
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h is not None and h.value:
+            try:
+                self._lib.jq_plan_free(h)
+            except Exception:  # pragma: no cover - interpreter shutdown
+                pass
+            self.handle = None
+
+    def workspace_bytes(self, batch: int, with_grad: int = 0) -> int:
+        return int(self._lib.jq_workspace_bytes(self.handle, batch, 0, with_grad))
+
+
+_PLAN_CACHE: "OrderedDict[tuple, Plan]" = OrderedDict()
+_PLAN_LOCK = threading.Lock()
+PLAN_CACHE_SIZE = 256
+
+
+def get_plan(lw: Lowered, obs_specs, obs_key, n_qubits: int, mode: int, dtype: torch.dtype,
+             tune: Optional[dict] = None) -> Plan:
+    key = (lw.key, obs_key, n_qubits, mode, dtype, tuple(sorted((tune or {}).items())))
+    with _PLAN_LOCK:
+        plan = _PLAN_CACHE.get(key)
+        if plan is not None:
+            _PLAN_CACHE.move_to_end(key)
+            return plan
+    plan = Plan(lw.statics, obs_specs, n_qubits, mode, dtype, tune)
+    with _PLAN_LOCK:
+        _PLAN_CACHE[key] = plan
+        while len(_PLAN_CACHE) > PLAN_CACHE_SIZE:
+            _PLAN_CACHE.popitem(last=False)
+    return plan
+
+
+def gather_angles(values: list, device: torch.device) -> Optional[torch.Tensor]:
+    """One float64 device tensor of the tape's angles (keeps autograd links)."""
+    if not values:
+        return None
+    tensors = [v for v in values if isinstance(v, torch.Tensor)]
+    if not tensors:
+        return torch.tensor([float(v) for v in values], dtype=torch.float64).to(device, non_blocking=True)
+    devs = {t.device for t in tensors}
+    home = tensors[0].device if len(devs) == 1 else device
+    parts = [
+        v.to(device=home, dtype=torch.float64).reshape(())
+        if isinstance(v, torch.Tensor)
+        else torch.tensor(float(v), dtype=torch.float64, device=home)
+        for v in values
+    ]
+    return torch.stack(parts).to(device)
+
+
+def gather_mats(values: list, device: torch.device) -> Optional[torch.Tensor]:
+    if not values:
+        return None
+    parts = [v.to(torch.complex128).reshape(-1).to(device) for v in values]
+    return torch.cat(parts) if len(parts) > 1 else parts[0]
+
+
+# ---------------------------------------------------------------------------
+# execution
+# ---------------------------------------------------------------------------
+def _ptr(t: Optional[torch.Tensor]):
+    return None if t is None else ctypes.c_void_p(t.data_ptr())
+
+
+def _stream() -> ctypes.c_void_p:
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+class _Execute(torch.autograd.Function):
+    """Forward = jq_forward; backward = jq_adjoint or jq_backward."""
+
+    @staticmethod
+    def forward(ctx, plan: Plan, out_type: int, batch: int, init_batched: int, angles, mats, init):
+        dev = _device()
+        lib = plan._lib
+        dim = 1 << plan.n_qubits
+        shape = (batch, dim, dim) if plan.mode == L.JQ_DENSITY else (batch, dim)
+        state = torch.empty(shape, dtype=plan.cdtype, device=dev)
+        out = None
+        if out_type == L.JQ_OUT_EXPVAL:
+            out = torch.empty((batch, plan.n_obs), dtype=torch.float64, device=dev)
+        elif out_type == L.JQ_OUT_PROBS:
+            out = torch.empty((batch, dim), dtype=plan.rdtype, device=dev)
+        elif out_type == L.JQ_OUT_DENSITY and plan.mode == L.JQ_STATEVECTOR:
+            out = torch.empty((batch, dim, dim), dtype=plan.cdtype, device=dev)
+        wsb = plan.workspace_bytes(batch, 0)
+        ws = torch.empty(max(wsb, 1), dtype=torch.uint8, device=dev)
+        L.check(
+            lib.jq_forward(
+                plan.handle, batch, _ptr(angles), _ptr(mats), _ptr(init), init_batched, out_type,
+                _ptr(state), _ptr(out), _ptr(ws), wsb, _stream(),
+            )
+        )
+        ctx.plan = plan
+        ctx.out_type = out_type
+        ctx.batch = batch
+        ctx.init_batched = init_batched
+        ctx.save_for_backward(angles, mats, init, state)
+        if out_type == L.JQ_OUT_STATE or (out_type == L.JQ_OUT_DENSITY and plan.mode == L.JQ_DENSITY):
+            return state
+        return out
+
+    @staticmethod
+    def backward(ctx, g):
+        plan: Plan = ctx.plan
+        angles, mats, init, state = ctx.saved_tensors
+        need_ang = angles is not None and ctx.needs_input_grad[4]
+        need_mat = mats is not None and ctx.needs_input_grad[5]
+        need_init = init is not None and ctx.needs_input_grad[6]
+        if not (need_ang or need_mat or need_init):
+            return None, None, None, None, None, None, None
+        dev = state.device
+        batch = ctx.batch
+        lib = plan._lib
+        g = g.contiguous()
+        ct = g if ctx.out_type == L.JQ_OUT_EXPVAL else None
+        ct_state = None if ctx.out_type == L.JQ_OUT_EXPVAL else g
+        if ct is not None:
+            ct = ct.to(torch.float64)
+        if ct_state is not None:
+            ct_state = ct_state.to(plan.rdtype if ctx.out_type == L.JQ_OUT_PROBS else plan.cdtype).contiguous()
+        ga = torch.empty((batch, plan.n_angles), dtype=torch.float64, device=dev) if need_ang else None
+        gm = torch.empty((batch, plan.n_mats), dtype=torch.complex128, device=dev) if need_mat else None
+        gi = torch.empty((batch, 1 << plan.n_qubits), dtype=plan.cdtype, device=dev) if need_init else None
+        use_adjoint = plan.mode == L.JQ_STATEVECTOR and plan.unitary
+        wsb = plan.workspace_bytes(batch, 1 if use_adjoint else 2)
+        ws = torch.empty(max(wsb, 1), dtype=torch.uint8, device=dev)
+        if use_adjoint:
+            L.check(
+                lib.jq_adjoint(
+                    plan.handle, batch, _ptr(angles), _ptr(mats), _ptr(state), ctx.out_type, _ptr(ct),
+                    _ptr(ct_state), _ptr(ga), _ptr(gm), _ptr(gi), _ptr(ws), wsb, _stream(),
+                )
+            )
+        else:
+            L.check(
+                lib.jq_backward(
+                    plan.handle, batch, _ptr(angles), _ptr(mats), _ptr(init), ctx.init_batched, ctx.out_type,
+                    _ptr(ct), _ptr(ct_state), _ptr(ga), _ptr(gm), _ptr(gi), _ptr(ws), wsb, _stream(),
+                )
+            )
+        if gi is not None and not ctx.init_batched:
+            gi = gi.sum(0)
+        if ga is not None and angles.dim() == 1:
+            ga = ga[0]
+        if gm is not None and mats.dim() == 1:
+            gm = gm[0]
+        return None, None, None, None, ga, gm, gi
+
+
+def run_plan(plan: Plan, out_type: int, batch: int, angles, mats, init, init_batched: int) -> torch.Tensor:
+    """Execute *plan* for *batch* instances through the autograd Function."""
+    return _Execute.apply(plan, out_type, batch, init_batched, angles, mats, init)
+
+
+def _prepare_init(initial_state, n_qubits: int, dtype: torch.dtype, device, batched_ok: bool):
+    if initial_state is None:
+        return None, 0
+    t = initial_state if isinstance(initial_state, torch.Tensor) else torch.as_tensor(np.asarray(initial_state))
+    t = t.to(device=device, dtype=dtype)
+    dim = 2**n_qubits
+    if t.dim() == 1:
+        if t.numel() != dim:
+            raise ValueError(f"initial_state has {t.numel()} amplitudes, expected {dim}")
+        return t.contiguous(), 0
+    if t.dim() == 2 and batched_ok:
+        if t.shape[1] != dim:
+            raise ValueError(f"initial_state rows have {t.shape[1]} amplitudes, expected {dim}")
+        return t.contiguous(), 1
+    raise ValueError(f"initial_state must be a 1D statevector; got ndim={t.dim()}.")
+
+
+def _resolve_dtype(dtype) -> torch.dtype:
+    if dtype is None:
+        return cdtype()
+    if dtype in (torch.complex64, "complex64", np.complex64):
+        return torch.complex64
+    if dtype in (torch.complex128, "complex128", np.complex128):
+        return torch.complex128
+    raise ValueError(f"unsupported dtype {dtype!r}")
+
+
+def _check_type(type: str, use_density: bool) -> None:
+    if type not in _TYPES:
+        raise ValueError(f"Unknown measurement type: {type!r}")
+    if use_density and type == "state":
+        raise ValueError(
+            "Measurement type 'state' is not defined for mixed (noisy) circuits. Use 'density' instead."
+        )
+
+
+def _finish(result: torch.Tensor, type: str, dtype: torch.dtype) -> torch.Tensor:
+    if type == "expval":
+        return result.to(rdtype(dtype))
+    return result
+
+
+def simulate_and_measure(
+    tape: List[Operation],
+    n_qubits: int,
+    type: str,
+    obs: List[Operation],
+    use_density: bool,
+    shots: Optional[int] = None,
+    key=None,
+    initial_state=None,
+    adjoint: bool = True,
+    dtype=None,
+    tune: Optional[dict] = None,
+) -> torch.Tensor:
+    """Simulate *tape* and measure (jaqsi/simulation.py:658-732).
+
+    ``adjoint`` is accepted for signature compatibility: the backward of a
+    unitary statevector plan is always the adjoint method, every other plan
+    uses the checkpointed reverse pass.  ``dtype`` selects complex64 or
+    complex128 (default :func:`~jaqsi_b200.operations.cdtype`).
+    """
+    obs = list(obs or [])
+    _check_type(type, use_density)
+    dt = _resolve_dtype(dtype)
+    dev = _device()
+    exact = shots is None or type not in ("probs", "expval")
+    mtype = type if exact else "probs"
+    mode = L.JQ_DENSITY if use_density else L.JQ_STATEVECTOR
+    lw = lower_tape(tape, n_qubits)
+    specs, okey = _lower_obs(obs if mtype == "expval" else [], n_qubits)
+    plan = get_plan(lw, specs, okey, n_qubits, mode, dt, tune)
+    angles = gather_angles(lw.angles, dev)
+    mats = gather_mats(lw.mats, dev)
+    init, init_b = _prepare_init(initial_state, n_qubits, dt, dev, batched_ok=False)
+    res = run_plan(plan, _OUT[mtype], 1, angles, mats, init, init_b)[0]
+    if not exact:
+        return sample_shots(res, n_qubits, type, obs, shots, key)
+    return _finish(res, type, dt)
+
+
+def measure_state(state: torch.Tensor, n_qubits: int, type: str, obs: List[Operation], dtype=None) -> torch.Tensor:
+    """Measure a given statevector (jaqsi/simulation.py:735-811).
+
+    Runs an empty plan on the GPU from *state*; differentiable w.r.t. the
+    state.  A leading batch dimension is allowed.
+    """
+    _check_type(type, False)
+    dt = _resolve_dtype(dtype if dtype is not None else (state.dtype if state.is_complex() else None))
+    dev = _device()
+    st = state if isinstance(state, torch.Tensor) else torch.as_tensor(np.asarray(state))
+    batched = st.dim() == 2
+    batch = st.shape[0] if batched else 1
+    st = st.reshape(batch, -1).to(device=dev, dtype=dt).contiguous()
+    lw = lower_tape([], n_qubits)
+    specs, okey = _lower_obs(obs if type == "expval" else [], n_qubits)
+    plan = get_plan(lw, specs, okey, n_qubits, L.JQ_STATEVECTOR, dt)
+    res = run_plan(plan, _OUT[type], batch, None, None, st, 1)
+    res = _finish(res, type, dt)
+    return res if batched else res[0]
+
+
+def measure_density(rho: torch.Tensor, n_qubits: int, type: str, obs: List[Operation], dtype=None) -> torch.Tensor:
+    """Measure a given density matrix (jaqsi/simulation.py:814-857)."""
+    if type not in _TYPES:
+        raise ValueError(f"Unknown measurement type: {type!r}")
+    if type == "state":
+        raise ValueError(
+            "Measurement type 'state' is not defined for mixed (noisy) circuits. Use 'density' instead."
+        )
+    dim = 2**n_qubits
+    r = rho if isinstance(rho, torch.Tensor) else torch.as_tensor(np.asarray(rho))
+    dt = _resolve_dtype(dtype if dtype is not None else (r.dtype if r.is_complex() else None))
+    r = r.to(dt)
+    if type == "density":
+        return r
+    if type == "probs":
+        return torch.real(torch.diagonal(r, dim1=-2, dim2=-1))
+    mats = torch.stack([ob.lifted_matrix(n_qubits).to(device=r.device, dtype=dt) for ob in obs])
+    return torch.real(torch.einsum("oij,...ji->...o", mats, r.reshape(*r.shape[:-2], dim, dim)))
+
+
+# ---------------------------------------------------------------------------
+# shots (jaqsi/simulation.py:860-917)
+# ---------------------------------------------------------------------------
+def _obs_diagonal(ob: Operation, n_qubits: int, device) -> torch.Tensor:
+    """diag of the lifted observable as a length-2^n real vector."""
+    dim = 2**n_qubits
+    idx = torch.arange(dim, device=device)
+    k = len(ob.wires)
+    sub = torch.zeros(dim, dtype=torch.long, device=device)
+    for i, w in enumerate(ob.wires):
+        sub = sub | (((idx >> (n_qubits - 1 - w)) & 1) << (k - 1 - i))
+    m = _concrete_matrix(ob) if not isinstance(ob, (PauliX, PauliY, PauliZ)) else type(ob)._matrix
+    d = torch.as_tensor(np.real(np.diag(np.asarray(m))).copy(), dtype=torch.float64, device=device)
+    return d[sub]
+
+
+def _generator(key, device) -> torch.Generator:
+    if isinstance(key, torch.Generator):
+        return key
+    g = torch.Generator(device=device)
+    g.manual_seed(0 if key is None else int(key))
+    return g
+
+
+def sample_shots(probs: torch.Tensor, n_qubits: int, type: str, obs, shots: int, key) -> torch.Tensor:
+    """Histogram of *shots* basis samples drawn from *probs* on the GPU.
+
+    ``key`` is an integer seed or a ``torch.Generator``; the draws are not the
+    reference's JAX PRNG stream, only the same distribution.
+    """
+    if type not in ("probs", "expval"):
+        raise ValueError(f"Shot simulation is only supported for 'probs' and 'expval', got {type!r}.")
+    dim = 2**n_qubits
+    p = probs.detach().to(torch.float64).clamp_min(0)
+    gen = _generator(key, p.device)
+    samples = torch.multinomial(p, shots, replacement=True, generator=gen)
+    counts = torch.bincount(samples, minlength=dim).to(torch.float64)
+    est = counts / shots
+    if type == "probs":
+        return est.to(probs.dtype)
+    vals = [torch.dot(_obs_diagonal(ob, n_qubits, p.device), est) for ob in obs]
+    return torch.stack(vals).to(probs.dtype) if vals else torch.zeros(0, dtype=probs.dtype, device=p.device)

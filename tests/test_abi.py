@@ -1,0 +1,156 @@
+"""The C ABI on CPU: exported symbols, struct layouts, the host planner's
+schedules and its error behaviour.  No kernel is launched here."""
+import ctypes
+import os
+import re
+import subprocess
+import tempfile
+
+import numpy as np
+import pytest
+import torch
+
+import jaqsi_b200 as jq
+from jaqsi_b200 import _lib as L
+from jaqsi_b200 import simulation as sim
+from oracle import sim_np as O
+from tests.helpers import ansatz_layers, random_circuit, to_records
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "jqsim.h")
+
+
+def _declared():
+    text = open(HEADER).read()
+    return sorted(set(re.findall(r"JQ_API\s+[\w\s\*]+?\b(jq_\w+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = L.lib()
+    declared = _declared()
+    assert len(declared) >= 10
+    for name in declared:
+        assert hasattr(lib, name), name
+    assert set(declared) == set(L.EXPORTED)
+    out = subprocess.run(["nm", "-D", L.LIB_PATH], capture_output=True, text=True, check=True).stdout
+    for name in declared:
+        assert re.search(rf"\bT {name}\b", out), name
+
+
+def test_struct_layouts_match_header(tmp_path):
+    src = tmp_path / "sz.c"
+    src.write_text(
+        '#include <stdio.h>\n#include <stddef.h>\n#include "jqsim.h"\n'
+        "int main(void){printf(\"%zu %zu %zu %zu %zu %zu\\n\", sizeof(jq_op), sizeof(jq_obs), sizeof(jq_tune),"
+        " sizeof(jq_plan_info), offsetof(jq_op, const_mat), offsetof(jq_obs, mat));return 0;}\n"
+    )
+    exe = tmp_path / "sz"
+    subprocess.run(["gcc", "-I", os.path.dirname(HEADER), str(src), "-o", str(exe)], check=True)
+    got = [int(v) for v in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
+    want = [ctypes.sizeof(L.JqOp), ctypes.sizeof(L.JqObs), ctypes.sizeof(L.JqTune), ctypes.sizeof(L.JqPlanInfo),
+            L.JqOp.const_mat.offset, L.JqObs.mat.offset]
+    assert got == want
+
+
+def _plan(tape, n, obs=(), mode=L.JQ_STATEVECTOR, dtype=torch.complex128, tune=None):
+    lw = sim.lower_tape(tape, n)
+    specs, _ = sim._lower_obs(list(obs), n)
+    return sim.Plan(lw.statics, specs, n, mode, dtype, tune)
+
+
+def _schedule(plan, which):
+    nb = plan.info["n_blocks"]
+    bp = (ctypes.c_int32 * max(nb, 1))()
+    bw = (ctypes.c_int32 * max(6 * nb, 1))()
+    L.check(plan._lib.jq_plan_block_passes(plan.handle, which, bp, bw, nb))
+    wires = [[w for w in bw[6 * b: 6 * b + 6] if w >= 0] for b in range(nb)]
+    return list(bp[:nb]), wires
+
+
+@pytest.mark.parametrize("which", [0, 1, 2])
+@pytest.mark.parametrize("n,seed", [(5, 0), (9, 1), (16, 2)])
+def test_schedule_respects_dependencies(n, seed, which):
+    """Every block is in exactly one pass, and blocks sharing a wire run in
+    program order (same pass: order kept inside the pass)."""
+    rng = np.random.default_rng(seed)
+    params = torch.linspace(0.1, 3.0, 2000, dtype=torch.float64)
+    with jq.recording() as tape:
+        random_circuit(n, 150, rng, params)
+    plan = _plan(tape, n)
+    bp, wires = _schedule(plan, which)
+    assert all(p >= 0 for p in bp)
+    last = {}
+    for b, ws in enumerate(wires):
+        for w in ws:
+            if w in last:
+                assert bp[last[w]] <= bp[b], (b, w)
+            last[w] = b
+    if which == 2:
+        assert len(set(bp)) == len(bp)
+
+
+def test_config2_pass_counts():
+    """24-qubit, 20-layer RX/RY/RZ + CX-ring sweep: jaqsi runs 500 passes
+    (restated _fuse/_fuse_runs), the tile schedule far fewer."""
+    n, layers = 24, 20
+    ang = np.random.default_rng(2).uniform(0, 2 * np.pi, (layers, n, 3))
+    with jq.recording() as tape:
+        ansatz_layers(n, layers, ang)
+    assert O.jaqsi_pass_count(to_records(tape)) == 500
+    for dt in (torch.complex64, torch.complex128):
+        info = _plan(tape, n, dtype=dt).info
+        assert info["n_blocks"] == 960
+        assert info["n_passes_fwd"] <= 60
+        assert info["n_tile_ops_fwd"] == 960
+
+
+def test_mixed_lowering_block_count():
+    """Density plans fuse gates with the channels on their wire, like
+    _compile_mixed (jaqsi/simulation.py:348-381)."""
+    n = 3
+    with jq.recording() as tape:
+        jq.RX(0.3, wires=0)
+        jq.DepolarizingChannel(0.1, wires=0)
+        jq.AmplitudeDamping(0.2, wires=0)
+        jq.RY(0.4, wires=0)
+        jq.CX(wires=[0, 1])
+    info = _plan(tape, n, mode=L.JQ_DENSITY).info
+    assert info["n_bits"] == 6
+    # one fused superoperator on (0, 3) and the CX on ket and bra wires
+    assert info["n_blocks"] == 3
+
+
+def test_invalid_inputs_raise():
+    with jq.recording() as tape:
+        jq.RX(0.1, wires=3)
+    with pytest.raises(ValueError):
+        sim.lower_tape(tape, 2)
+    with jq.recording() as tape:
+        jq.BitFlip(0.1, wires=0)
+    lw = sim.lower_tape(tape, 1)
+    with pytest.raises(ValueError, match="noise channel"):
+        sim.Plan(lw.statics, [], 1, L.JQ_STATEVECTOR, torch.complex128)
+    with pytest.raises(ValueError):
+        jq.CX(wires=[0, 0])
+    with pytest.raises(ValueError):
+        jq.RX(0.1, wires=[0, 1])
+    with pytest.raises(ValueError, match="Unknown measurement type"):
+        sim._check_type("nope", False)
+    with pytest.raises(ValueError, match="not defined for mixed"):
+        sim._check_type("state", True)
+
+
+def test_no_gpu_fails_loudly(monkeypatch):
+    """The product has no CPU fallback."""
+    monkeypatch.setattr(torch.cuda, "is_available", lambda: False)
+    with pytest.raises(RuntimeError, match="CUDA"):
+        jq.Script(lambda: jq.H(0), 1).execute("probs")
+
+
+def test_pauli_detection():
+    m = np.kron(O.Z, O.Y) * 2.0
+    assert sim._detect_pauli(m) == (0b01, 0b11, 1, 2.0)
+    assert sim._detect_pauli(O.HAD) is None
+    specs, _ = sim._lower_obs([jq.build_parity_observable([0, 2]), jq.PauliX(1)], 3)
+    assert specs[0][:5] == ("P", 0, 0b101, 0, 1.0)
+    assert specs[1][:5] == ("P", 0b010, 0, 0, 1.0)
