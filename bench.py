@@ -1,0 +1,389 @@
+#!/usr/bin/env python
+"""Benchmark of the jaqsi circuit-execution hot path on B200.
+
+Default workload (N=1): the 24-qubit forward gate sweep in complex64 — 20
+layers of RX/RY/RZ on every wire plus a CX ring (i -> i+1 mod n), seeded
+uniform angles in [0, 2pi), |0..0>, expectation values of Z_i Z_{i+1} for the
+open chain i = 0..22.  One step = one forward sweep + measurement.
+
+  value   gate-pass GB/s with inputs resident in HBM, counted as the
+          reference's plan executes the step: P_ref passes (jaqsi's fused plan,
+          500 here) x 2 x 2^n x 8 B, divided by the measured step time.  This is
+          the reference's per-step HBM traffic per second of our step time.
+  roofline  the dominant kernel (the tile pass): its own algorithmic bytes per
+          launch (one read + one write of the state) over its average launch
+          duration, against the measured HBM copy bandwidth.
+  e2e     same metric through the public API (Script.execute) with the angles
+          in host memory and the expectation values copied back every step.
+  cpu_baseline / --impl reference: the reference plan executed by the oracle's
+          OpenMP C restatement on the host cores (jaqsi itself runs on JAX,
+          which is not installed on these machines).
+
+Multi-GPU: single circuits do not shard, so N GPUs run N replicas
+(weak scaling), timed as the max over ranks.
+"""
+import argparse
+import ctypes
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "adjoint grads/sec (batched) vs plain GPU sim at ≤1e-5 err; gate-pass HBM GB/s"
+N_QUBITS, LAYERS, SEED = 24, 20, 2
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def _angles():
+    return np.random.default_rng(SEED).uniform(0, 2 * np.pi, (LAYERS, N_QUBITS, 3))
+
+
+def _records(ang):
+    recs = []
+    for l in range(LAYERS):
+        for w in range(N_QUBITS):
+            recs += [("RX", [w], [ang[l, w, 0]]), ("RY", [w], [ang[l, w, 1]]), ("RZ", [w], [ang[l, w, 2]])]
+        recs += [("CX", [w, (w + 1) % N_QUBITS], []) for w in range(N_QUBITS)]
+    return recs
+
+
+class Clocks:
+    """nvidia-smi samples of the SM clock and throttle reasons while timing."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def __enter__(self):
+        def run():
+            q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+                 "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_power_cap")
+            while not self._stop.is_set():
+                try:
+                    out = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                         timeout=5).stdout.strip()
+                    if out:
+                        self.rows.append([v.strip() for v in out.split(",")])
+                except Exception:
+                    pass
+                self._stop.wait(0.2)
+
+        self._t = threading.Thread(target=run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *exc):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if len(r) > 3 + i and r[3 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+_REF_CACHE = {}
+
+
+def cpu_reference(layers_sample: int, dtype: str):
+    """Time the reference plan (oracle C restatement, all host cores) on the
+    first `layers_sample` layers and scale to the full sweep + measurement."""
+    from oracle import sim_np as O
+
+    lib_path = os.path.join(ROOT, "oracle", "_build", "libjqoracle.so")
+    if not os.path.exists(lib_path):
+        subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle")], check=True)
+    lib = ctypes.CDLL(lib_path)
+    f = "f" if dtype == "c64" else ""
+    T = ctypes.c_float if dtype == "c64" else ctypes.c_double
+    npd = np.float32 if dtype == "c64" else np.float64
+    for name in ("dense", "gather", "diag", "init_zero"):
+        getattr(lib, f"jqo_{name}{f}").restype = None
+    getattr(lib, f"jqo_expval_z{f}").restype = ctypes.c_double
+    n = N_QUBITS
+    ang = _angles()
+    key = (layers_sample, dtype)
+    if key not in _REF_CACHE:
+        # the reference plan of the first layers is the prefix of the full plan:
+        # each layer ends with one composed CX-ring permutation entry
+        sample = [r for r in _records(ang)][: layers_sample * 4 * N_QUBITS]
+        _REF_CACHE[key] = (O.jaqsi_plan(sample, n), O.jaqsi_pass_count(_records(ang)))
+    plan, p_ref = _REF_CACHE[key]
+    psi = np.zeros(2 * (1 << n), dtype=npd)
+    tmp = np.zeros_like(psi)
+    P = ctypes.POINTER(T)
+    pp, tp = psi.ctypes.data_as(P), tmp.ctypes.data_as(P)
+    entries = []
+    for e in plan:
+        if e[0] == "dense":
+            w = (ctypes.c_int * len(e[1]))(*e[1])
+            m = np.ascontiguousarray(e[2], dtype=np.complex128).view(np.float64)
+            entries.append(("dense", len(e[1]), w, m))
+        elif e[0] == "gather":
+            entries.append(("gather", np.ascontiguousarray(e[1], dtype=np.int32)))
+        else:
+            w = (ctypes.c_int * len(e[1]))(*e[1])
+            entries.append(("diag", len(e[1]), w, np.ascontiguousarray(e[2], dtype=np.complex128).view(np.float64)))
+    dp = ctypes.POINTER(ctypes.c_double)
+    zmasks = [(1 << (n - 1 - i)) | (1 << (n - 2 - i)) for i in range(n - 1)]
+    getattr(lib, f"jqo_init_zero{f}")(pp, n)
+    t0 = time.perf_counter()
+    for e in entries:
+        if e[0] == "dense":
+            getattr(lib, f"jqo_dense{f}")(pp, n, e[1], e[2], e[3].ctypes.data_as(dp))
+        elif e[0] == "gather":
+            getattr(lib, f"jqo_gather{f}")(pp, tp, n, e[1].ctypes.data_as(ctypes.POINTER(ctypes.c_int32)))
+        else:
+            getattr(lib, f"jqo_diag{f}")(pp, n, e[1], e[2], e[3].ctypes.data_as(dp))
+    t1 = time.perf_counter()
+    ev = [getattr(lib, f"jqo_expval_z{f}")(pp, n, ctypes.c_uint64(z)) for z in zmasks]
+    t2 = time.perf_counter()
+    sweep_s = (t1 - t0) * LAYERS / layers_sample
+    step_s = sweep_s + (t2 - t1)
+    cores = len(os.sched_getaffinity(0))
+    threads = lib.jqo_max_threads()
+    return step_s, p_ref, cores, threads, ev
+
+
+def reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    pass_bytes = 2 * (1 << N_QUBITS) * (8 if args.dtype == "c64" else 16)
+    times = []
+    for _ in range(args.warmup):
+        cpu_reference(args.sample_layers, args.dtype)
+    for _ in range(args.steps):
+        s, p_ref, cores, threads, _ = cpu_reference(args.sample_layers, args.dtype)
+        times.append(s)
+    step = statistics.median(times)
+    value = p_ref * pass_bytes / step / 1e9
+    sample = (f"reference plan ({p_ref} passes) of the {N_QUBITS}-qubit {LAYERS}-layer sweep: first "
+              f"{args.sample_layers} layers timed per step and scaled x{LAYERS / args.sample_layers:g}, "
+              f"plus the {N_QUBITS - 1} ZZ expectation values")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": step * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": args.dtype, "data": "synthetic (seeded angles)",
+        "config": _config(args, p_ref, None),
+        "cpu_baseline": {"value": value, "unit": "GB/s", "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def _config(args, p_ref, p_ours):
+    return {
+        "workload": f"forward gate sweep, {N_QUBITS}-qubit statevector, {LAYERS} layers of RX/RY/RZ on every "
+                    f"wire + CX ring, expval of Z_iZ_(i+1) (open chain)",
+        "n_qubits": N_QUBITS, "layers": LAYERS, "seed": SEED, "dtype": args.dtype,
+        "reference_plan_passes": p_ref, "our_passes": p_ours,
+        "value_def": "reference-plan passes x 2 x 2^n x elem bytes / step time",
+        "l2": "flushed between timed steps (256 MiB write); state 128 MiB (c64) / 256 MiB (c128)",
+        "parallelism": f"replicas x{args.gpus}",
+    }
+
+
+def ours_arm(args):
+    import torch
+    import torch.distributed as dist
+
+    import jaqsi_b200 as jq
+    from jaqsi_b200 import _lib as L
+    from jaqsi_b200 import simulation as sim
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=dev)
+    dt = torch.complex64 if args.dtype == "c64" else torch.complex128
+    elem = 8 if args.dtype == "c64" else 16
+    n = N_QUBITS
+    ang = _angles()
+    ang_t = torch.tensor(ang)
+
+    def circuit(a):
+        for l in range(LAYERS):
+            for w in range(n):
+                jq.RX(a[l, w, 0], wires=w)
+                jq.RY(a[l, w, 1], wires=w)
+                jq.RZ(a[l, w, 2], wires=w)
+            for w in range(n):
+                jq.CX(wires=[w, (w + 1) % n])
+
+    obs = [jq.build_parity_observable([i, i + 1]) for i in range(n - 1)]
+    script = jq.Script(circuit, n_qubits=n)
+    tape = script.record(ang_t)
+    lw = sim.lower_tape(tape, n)
+    specs, okey = sim._lower_obs(obs, n)
+    tune = {"tile_bits": args.tile_bits} if args.tile_bits else None
+    plan = sim.get_plan(lw, specs, okey, n, L.JQ_STATEVECTOR, dt, tune)
+    from oracle import sim_np as O
+
+    p_ref = O.jaqsi_pass_count(_records(ang))
+    P = plan.info["n_passes_fwd"]
+    angles = sim.gather_angles(lw.angles, dev)
+    state = torch.empty((1, plan.state_elems), dtype=dt, device=dev)
+    out = torch.empty((1, plan.n_obs), dtype=torch.float64, device=dev)
+    wsb = plan.workspace_bytes(1, 0)
+    ws = torch.empty(max(wsb, 1), dtype=torch.uint8, device=dev)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+    lib = plan._lib
+    stream = torch.cuda.current_stream()
+    sp = ctypes.c_void_p(stream.cuda_stream)
+    vp = ctypes.c_void_p
+
+    def fwd():
+        L.check(lib.jq_forward(plan.handle, 1, vp(angles.data_ptr()), None, None, 0, L.JQ_OUT_EXPVAL,
+                               vp(state.data_ptr()), vp(out.data_ptr()), vp(ws.data_ptr()), wsb, sp))
+
+    def sweep():
+        L.check(lib.jq_sweep(plan.handle, 1, vp(angles.data_ptr()), None, vp(state.data_ptr()),
+                             vp(ws.data_ptr()), wsb, sp))
+
+    def timed(fn, steps):
+        total = 0.0
+        for _ in range(steps):
+            flush.zero_()
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            fn()
+            b.record(stream)
+            b.synchronize()
+            total += a.elapsed_time(b)
+        return total / steps
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    for _ in range(args.warmup):
+        fwd()
+        sweep()
+    barrier()
+    with Clocks(local) as clk:
+        step_ms = max_over_ranks(timed(fwd, args.steps))
+        barrier()
+        sweep_ms = max_over_ranks(timed(sweep, args.steps))
+        barrier()
+    ev = out[0].detach().cpu().numpy()
+
+    # e2e through the public API: host angles in, expectation values out
+    def e2e_step():
+        res = sim.simulate_and_measure(script.record(ang_t), n, "expval", obs, False, dtype=dt, tune=tune)
+        return res.cpu()
+
+    for _ in range(max(1, args.warmup)):
+        e2e_step()
+    barrier()
+    e2e_total = 0.0
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        e2e_step()
+        b.record(stream)
+        b.synchronize()
+        e2e_total += a.elapsed_time(b)
+    e2e_ms = max_over_ranks(e2e_total / args.steps)
+    barrier()
+
+    pass_bytes = 2 * (1 << n) * elem
+    value = world * p_ref * pass_bytes / (step_ms * 1e-3) / 1e9
+    e2e_value = world * p_ref * pass_bytes / (e2e_ms * 1e-3) / 1e9
+    peak, peak_kind = _peaks()
+    achieved = P * pass_bytes / (sweep_ms * 1e-3) / 1e9
+    n_obs_chunks = math.ceil(plan.n_obs / 16)
+    launches = (2 + P + n_obs_chunks) * args.steps
+    result = {
+        "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": args.dtype, "data": "synthetic (seeded angles, |0..0>)",
+        "config": _config(args, p_ref, P),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
+                     "kernel": "k_tile_fwd", "launches_per_step": P,
+                     "avg_launch_us": sweep_ms * 1e3 / P, "bytes_per_launch": pass_bytes},
+        "e2e": {"value": e2e_value, "unit": "GB/s", "ms_per_step": e2e_ms,
+                "h2d_bytes_per_step": int(plan.n_angles * 8), "d2h_bytes_per_step": int(plan.n_obs * elem // 2)},
+        "gpu_launches": launches,
+        "clocks": clk.summary(),
+        "expval_sum": float(ev.sum()),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu:
+        s, _, cores, threads, cev = cpu_reference(args.sample_layers, args.dtype)
+        result["cpu_baseline"] = {
+            "value": p_ref * pass_bytes / s / 1e9, "unit": "GB/s", "cores": threads, "kind": "port",
+            "sample": f"reference plan, first {args.sample_layers} of {LAYERS} layers timed and scaled",
+            "ms_per_step": s * 1e3,
+        }
+    if rank == 0:
+        print(json.dumps(result))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--dtype", default="c64", choices=["c64", "c128"])
+    ap.add_argument("--sample-layers", type=int, default=2)
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--tile-bits", type=int, default=0, help="override the forward tile size (qubits per CTA)")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return reference_arm(args)
+    return ours_arm(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -127,6 +127,9 @@ typedef struct jq_tune {
   int32_t no_fuse;       /* nonzero: one pass per gate block (unfused baseline) */
   int32_t ckpt_stride;   /* passes between checkpoints of the checkpointed
                             reverse pass (0: ceil(sqrt(passes)))             */
+  int32_t jit;           /* forward passes specialised per plan with NVRTC:
+                            0 auto (states of >= 2^16 amplitudes), 1 on,
+                            -1 off (register-stage interpreter only)          */
 } jq_tune;
 
 /* Plan summary. */
@@ -145,6 +148,8 @@ typedef struct jq_plan_info {
   int32_t n_obs;
   int32_t unitary;         /* every op unitary (adjoint allowed)             */
   int64_t state_elems;     /* complex elements of one state (2^n or 4^n)     */
+  int32_t n_stages_fwd;    /* register stages over all forward passes        */
+  int32_t n_smem_ops_fwd;  /* generic shared-memory steps of the forward     */
 } jq_plan_info;
 
 typedef struct jq_plan jq_plan;
@@ -168,6 +173,11 @@ JQ_API int jq_plan_get_info(const jq_plan* plan, jq_plan_info* info);
 JQ_API int jq_plan_block_passes(const jq_plan* plan, int which, int32_t* block_pass,
                                 int32_t* block_wires, int n);
 
+/* CUDA C++ source of the plan's per-plan specialised forward passes (see
+ * jq_tune.jit), written to buf (NUL-terminated, truncated to n bytes);
+ * returns the full length.  Diagnostic; no reference counterpart. */
+JQ_API size_t jq_plan_jit_source(const jq_plan* plan, char* buf, size_t n);
+
 /* Device workspace (bytes) for `batch` instances: with_grad 0 sizes
  * jq_forward, 1 sizes jq_adjoint, 2 sizes jq_backward. */
 JQ_API size_t jq_workspace_bytes(const jq_plan* plan, int batch, int out_type,
@@ -190,6 +200,15 @@ JQ_API int jq_forward(const jq_plan* plan, int batch, const double* angles,
                const void* mats, const void* init, int init_batched,
                int out_type, void* state, void* out, void* workspace,
                size_t workspace_bytes, void* stream);
+
+/* Forward gate sweep of a statevector / density plan applied in place to a
+ * resident state (no initialisation, no measurement): the state after
+ * jq_sweep equals simulate_pure's result for `state` as initial state.
+ * Replaces jaqsi/simulation.py:400-409 (_run) for a caller that keeps the
+ * state on the device between circuit segments. */
+JQ_API int jq_sweep(const jq_plan* plan, int batch, const double* angles,
+                    const void* mats, void* state, void* workspace,
+                    size_t workspace_bytes, void* stream);
 
 /* Adjoint-method gradient of the expectation values of a unitary pure-state
  * plan, O(1) extra statevectors.  Replaces jaqsi/simulation.py:546-655

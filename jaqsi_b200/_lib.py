@@ -43,8 +43,10 @@ EXPORTED = (
     "jq_plan_free",
     "jq_plan_get_info",
     "jq_plan_block_passes",
+    "jq_plan_jit_source",
     "jq_workspace_bytes",
     "jq_forward",
+    "jq_sweep",
     "jq_adjoint",
     "jq_backward",
     "jq_last_error",
@@ -93,6 +95,7 @@ class JqTune(ctypes.Structure):
         ("threads", ctypes.c_int32),
         ("no_fuse", ctypes.c_int32),
         ("ckpt_stride", ctypes.c_int32),
+        ("jit", ctypes.c_int32),
     ]
 
 
@@ -114,6 +117,8 @@ class JqPlanInfo(ctypes.Structure):
         ("n_obs", ctypes.c_int32),
         ("unitary", ctypes.c_int32),
         ("state_elems", ctypes.c_int64),
+        ("n_stages_fwd", ctypes.c_int32),
+        ("n_smem_ops_fwd", ctypes.c_int32),
     ]
 
     def as_dict(self) -> dict:
@@ -139,10 +144,14 @@ def _declare(lib: ctypes.CDLL) -> None:
     lib.jq_plan_get_info.restype = i32
     lib.jq_plan_block_passes.argtypes = [vp, i32, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32), i32]
     lib.jq_plan_block_passes.restype = i32
+    lib.jq_plan_jit_source.argtypes = [vp, ctypes.c_char_p, ctypes.c_size_t]
+    lib.jq_plan_jit_source.restype = ctypes.c_size_t
     lib.jq_workspace_bytes.argtypes = [vp, i32, i32, i32]
     lib.jq_workspace_bytes.restype = ctypes.c_size_t
     lib.jq_forward.argtypes = [vp, i32, vp, vp, vp, i32, i32, vp, vp, vp, ctypes.c_size_t, vp]
     lib.jq_forward.restype = i32
+    lib.jq_sweep.argtypes = [vp, i32, vp, vp, vp, vp, ctypes.c_size_t, vp]
+    lib.jq_sweep.restype = i32
     lib.jq_adjoint.argtypes = [vp, i32, vp, vp, vp, i32, vp, vp, vp, vp, vp, vp, ctypes.c_size_t, vp]
     lib.jq_adjoint.restype = i32
     lib.jq_backward.argtypes = [vp, i32, vp, vp, vp, i32, i32, vp, vp, vp, vp, vp, vp, ctypes.c_size_t, vp]

@@ -10,7 +10,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libjqsim.so")
-SOURCES = ["planner.cpp", "jqsim.cu"]
+SOURCES = ["planner.cpp", "jit.cpp", "jqsim.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -38,7 +38,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
         "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
         "--expt-relaxed-constexpr", "-I", os.path.join(HERE, "..", "include"),
         *[os.path.join(CSRC, s) for s in SOURCES],
-        "-o", LIB + ".tmp", "-lcudart",
+        "-o", LIB + ".tmp", "-lcudart", "-ldl",
     ]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")

@@ -1,0 +1,478 @@
+// Per-plan specialisation of the forward tile passes.
+//
+// The register-stage interpreter (k_tile_fwd2 in jqsim.cu) decodes every op
+// at run time; for a plan that will be executed many times the pass programs
+// are instead emitted as straight-line CUDA C++ (literal shared-memory
+// offsets, gate bodies unrolled over named registers, basis permutations such
+// as CX folded into register renames at generation time) and compiled once
+// per plan and device with NVRTC for sm_100a.  Gate matrices stay run-time
+// data (staged in shared memory per tile), so one compiled plan serves every
+// parameter set of the same circuit structure, like the reference caches one
+// compiled executable per circuit signature (jaqsi/script.py:695-725).
+//
+// NVRTC and the driver entry points are resolved at run time (dlopen /
+// cudaGetDriverEntryPoint); without them the interpreter kernel runs instead.
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <dlfcn.h>
+#include <nvrtc.h>
+
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "jit.h"
+
+namespace jq {
+void set_error(const std::string& msg);
+
+namespace {
+
+// ---- run-time bindings ------------------------------------------------------
+struct Nvrtc {
+  bool ok = false;
+  nvrtcResult (*create)(nvrtcProgram*, const char*, const char*, int, const char* const*, const char* const*);
+  nvrtcResult (*compile)(nvrtcProgram, int, const char* const*);
+  nvrtcResult (*log_size)(nvrtcProgram, size_t*);
+  nvrtcResult (*log)(nvrtcProgram, char*);
+  nvrtcResult (*cubin_size)(nvrtcProgram, size_t*);
+  nvrtcResult (*cubin)(nvrtcProgram, char*);
+  nvrtcResult (*destroy)(nvrtcProgram*);
+};
+
+struct Driver {
+  bool ok = false;
+  CUresult (*module_load)(CUmodule*, const void*);
+  CUresult (*module_unload)(CUmodule);
+  CUresult (*get_function)(CUfunction*, CUmodule, const char*);
+  CUresult (*launch)(CUfunction, unsigned, unsigned, unsigned, unsigned, unsigned, unsigned, unsigned, CUstream,
+                     void**, void**);
+  CUresult (*set_attr)(CUfunction, CUfunction_attribute, int);
+  CUresult (*occupancy)(int*, CUfunction, int, size_t);
+};
+
+std::once_flag g_once;
+Nvrtc g_nvrtc;
+Driver g_drv;
+
+template <typename F>
+bool sym(void* h, const char* name, F* out) {
+  *out = reinterpret_cast<F>(dlsym(h, name));
+  return *out != nullptr;
+}
+
+template <typename F>
+bool entry(const char* name, F* out) {
+  void* p = nullptr;
+  cudaDriverEntryPointQueryResult q;
+  if (cudaGetDriverEntryPoint(name, &p, cudaEnableDefault, &q) != cudaSuccess || q != cudaDriverEntryPointSuccess)
+    return false;
+  *out = reinterpret_cast<F>(p);
+  return true;
+}
+
+void init_bindings() {
+  const char* names[] = {"libnvrtc.so.12", "libnvrtc.so", "/usr/local/cuda/lib64/libnvrtc.so.12"};
+  void* h = nullptr;
+  for (const char* n : names)
+    if ((h = dlopen(n, RTLD_NOW | RTLD_LOCAL))) break;
+  if (h) {
+    g_nvrtc.ok = sym(h, "nvrtcCreateProgram", &g_nvrtc.create) && sym(h, "nvrtcCompileProgram", &g_nvrtc.compile) &&
+                 sym(h, "nvrtcGetProgramLogSize", &g_nvrtc.log_size) && sym(h, "nvrtcGetProgramLog", &g_nvrtc.log) &&
+                 sym(h, "nvrtcGetCUBINSize", &g_nvrtc.cubin_size) && sym(h, "nvrtcGetCUBIN", &g_nvrtc.cubin) &&
+                 sym(h, "nvrtcDestroyProgram", &g_nvrtc.destroy);
+  }
+  g_drv.ok = entry("cuModuleLoadData", &g_drv.module_load) && entry("cuModuleUnload", &g_drv.module_unload) &&
+             entry("cuModuleGetFunction", &g_drv.get_function) && entry("cuLaunchKernel", &g_drv.launch) &&
+             entry("cuFuncSetAttribute", &g_drv.set_attr) &&
+             entry("cuOccupancyMaxActiveBlocksPerMultiprocessor", &g_drv.occupancy);
+}
+
+// ---- device prelude shared by every generated kernel --------------------------
+const char* kPrelude = R"JQ(
+typedef unsigned int u32;
+typedef unsigned long long u64;
+template <typename C> __device__ __forceinline__ C cmul(C a, C b) {
+  C r; r.x = a.x * b.x - a.y * b.y; r.y = a.x * b.y + a.y * b.x; return r;
+}
+template <typename C> __device__ __forceinline__ C cfma(C a, C b, C acc) {
+  C r; r.x = fma(a.x, b.x, fma(-a.y, b.y, acc.x)); r.y = fma(a.x, b.y, fma(a.y, b.x, acc.y)); return r;
+}
+__device__ __forceinline__ u64 pdep64(u64 v, u64 mask) {
+  u64 r = 0;
+  for (u64 bb = 1; mask; bb <<= 1) { u64 low = mask & (~mask + 1); if (v & bb) r |= low; mask &= mask - 1; }
+  return r;
+}
+__device__ __forceinline__ u32 swz8(u32 l) { return l ^ (((l >> 4) ^ (l >> 8) ^ (l >> 12)) & 15u); }
+__device__ __forceinline__ u32 swz16(u32 l) { return l ^ (((l >> 3) ^ (l >> 6) ^ (l >> 9) ^ (l >> 12)) & 7u); }
+template <int B>
+__device__ __forceinline__ void load8(float2* s, const float2* g, const u32* tbl, int t, int c) {
+  const int cm = (1 << c) - 1, nv = (1 << t) / 2;
+  for (int v0 = threadIdx.x; v0 < nv; v0 += B * blockDim.x) {
+    float4 r[B];
+#pragma unroll
+    for (int u = 0; u < B; ++u) { const int v = v0 + u * blockDim.x; if (v < nv) { const int l = 2 * v; r[u] = __ldcs((const float4*)(g + (tbl[l >> c] | (l & cm)))); } }
+#pragma unroll
+    for (int u = 0; u < B; ++u) { const int v = v0 + u * blockDim.x; if (v < nv) { const u32 l = 2 * v; s[swz8(l)] = make_float2(r[u].x, r[u].y); s[swz8(l + 1)] = make_float2(r[u].z, r[u].w); } }
+  }
+}
+template <int B>
+__device__ __forceinline__ void store8(const float2* s, float2* g, const u32* tbl, int t, int c) {
+  const int cm = (1 << c) - 1, nv = (1 << t) / 2;
+  for (int v0 = threadIdx.x; v0 < nv; v0 += B * blockDim.x) {
+    float4 r[B];
+#pragma unroll
+    for (int u = 0; u < B; ++u) { const int v = v0 + u * blockDim.x; if (v < nv) { const u32 l = 2 * v; const float2 a = s[swz8(l)], b = s[swz8(l + 1)]; r[u] = make_float4(a.x, a.y, b.x, b.y); } }
+#pragma unroll
+    for (int u = 0; u < B; ++u) { const int v = v0 + u * blockDim.x; if (v < nv) { const int l = 2 * v; __stcs((float4*)(g + (tbl[l >> c] | (l & cm))), r[u]); } }
+  }
+}
+template <int B>
+__device__ __forceinline__ void load16(double2* s, const double2* g, const u32* tbl, int t, int c) {
+  const int cm = (1 << c) - 1, nv = 1 << t;
+  for (int v0 = threadIdx.x; v0 < nv; v0 += B * blockDim.x) {
+    double2 r[B];
+#pragma unroll
+    for (int u = 0; u < B; ++u) { const int v = v0 + u * blockDim.x; if (v < nv) r[u] = __ldcs(g + (tbl[v >> c] | (v & cm))); }
+#pragma unroll
+    for (int u = 0; u < B; ++u) { const int v = v0 + u * blockDim.x; if (v < nv) s[swz16(v)] = r[u]; }
+  }
+}
+template <int B>
+__device__ __forceinline__ void store16(const double2* s, double2* g, const u32* tbl, int t, int c) {
+  const int cm = (1 << c) - 1, nv = 1 << t;
+  for (int v0 = threadIdx.x; v0 < nv; v0 += B * blockDim.x) {
+    double2 r[B];
+#pragma unroll
+    for (int u = 0; u < B; ++u) { const int v = v0 + u * blockDim.x; if (v < nv) r[u] = s[swz16(v)]; }
+#pragma unroll
+    for (int u = 0; u < B; ++u) { const int v = v0 + u * blockDim.x; if (v < nv) __stcs(g + (tbl[v >> c] | (v & cm)), r[u]); }
+  }
+}
+)JQ";
+
+std::string hex(uint64_t v) {
+  char b[32];
+  std::snprintf(b, sizeof(b), "0x%llxull", static_cast<unsigned long long>(v));
+  return b;
+}
+
+// Emit the kernel of pass p (register-stage program only).
+void emit_pass(std::ostringstream& o, const jq_plan* plan, const Schedule& s, int p, bool c64, int rb) {
+  const PassDesc& pd = s.passes[p];
+  const char* T = c64 ? "float2" : "double2";
+  const int t = pd.t, c = pd.c, nb = plan->n_bits;
+  const int nthr = 1 << (t - rb);
+  const int nr = 1 << rb;
+  const int minb = std::max(1, std::min(8, 65536 / (nthr * 128)));
+  const uint64_t full = (nb >= 64) ? ~0ULL : ((1ULL << nb) - 1);
+  const uint64_t outer = full & ~pd.tile_mask;
+  const int smat_pad = (pd.smat_len + 1) & ~1;
+  int nmc = 0;
+  for (int ri = pd.rop_begin; ri < pd.rop_end; ++ri) nmc += s.rops[ri].mat_len > 0;
+  o << "extern \"C\" __global__ void __launch_bounds__(" << nthr << ", " << minb << ") @KERNEL@(" << T
+    << "* __restrict__ state, int batch, const " << T << "* __restrict__ bmat, long long bstride, "
+    << "const int* __restrict__ mc) {\n";
+  o << "  extern __shared__ __align__(16) unsigned char smem[];\n";
+  o << "  " << T << "* s = (" << T << "*)smem;\n";
+  o << "  " << T << "* smat = s + " << (1 << t) << ";\n";
+  o << "  u32* tbl = (u32*)(smat + " << smat_pad << ");\n";
+  o << "  const u32 tid = threadIdx.x;\n";
+  // bit-deposit table of the tile's high bits
+  o << "  { const u32 hb[] = {";
+  for (int i = c; i < t; ++i) o << (i > c ? ", " : "") << (1u << pd.bits[i]);
+  if (t == c) o << "0u";
+  o << "};\n    for (int h = tid; h < " << (1 << (t - c)) << "; h += blockDim.x) { u32 v = 0;";
+  o << " for (int i = 0; i < " << (t - c) << "; ++i) if ((h >> i) & 1) v |= hb[i]; tbl[h] = v; } }\n";
+  // per-stage thread bases (tile independent)
+  int nstage = 0;
+  for (int si = pd.step_begin; si < pd.step_end; ++si) {
+    const Step& st = s.steps[si];
+    o << "  u32 tb" << nstage << " = 0;";
+    for (int i = 0; i < t - rb; ++i) o << " if (tid & " << (1u << i) << "u) tb" << nstage << " ^= " << st.tbits[i] << "u;";
+    o << "\n";
+    ++nstage;
+  }
+  o << "  const long long tiles_per = 1ll << " << (nb - t) << ";\n";
+  o << "  const long long ntiles = tiles_per * batch;\n";
+  o << "  long long last_inst = -1;\n";
+  o << "  for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {\n";
+  o << "    const long long inst = tile >> " << (nb - t) << ";\n";
+  o << "    const u64 ti = (u64)tile & (u64)(tiles_per - 1);\n";
+  o << "    " << T << "* g = state + (inst << " << nb << ") + pdep64(ti, " << hex(outer) << ");\n";
+  o << "    __syncthreads();\n";
+  // gate matrices of this pass: mc holds (smem offset, block-matrix offset,
+  // length) per matrix, so passes that differ only in their gates share code
+  o << "    if (inst != last_inst) {\n      const " << T << "* bm = bmat + inst * bstride;\n";
+  o << "      for (int i = 0; i < " << nmc << "; ++i) { const int d = mc[3 * i], a = mc[3 * i + 1], n = mc[3 * i + 2];\n";
+  o << "        for (int e = tid; e < n; e += blockDim.x) smat[d + e] = bm[a + e]; }\n";
+  o << "      (void)bm; last_inst = inst;\n    }\n";
+  o << "    " << (c64 ? "load8<4>" : "load16<2>") << "(s, g, tbl, " << t << ", " << c << ");\n";
+  o << "    __syncthreads();\n";
+  nstage = 0;
+  for (int si = pd.step_begin; si < pd.step_end; ++si) {
+    const Step& st = s.steps[si];
+    // address of register slot j
+    std::vector<uint32_t> off(nr);
+    for (int j = 0; j < nr; ++j) {
+      uint32_t a = 0;
+      for (int q = 0; q < rb; ++q)
+        if ((j >> q) & 1) a ^= st.ebits[q];
+      off[j] = a;
+    }
+    std::vector<int> var(nr);  // var[j]: variable holding amplitude j of the register block
+    for (int j = 0; j < nr; ++j) var[j] = j;
+    o << "    {\n";
+    for (int j = 0; j < nr; ++j) o << "      " << T << " v" << j << " = s[tb" << nstage << " ^ " << off[j] << "u];\n";
+    for (int ri = st.a; ri < st.b; ++ri) {
+      const RegOp& ro = s.rops[ri];
+      const uint32_t kind = ro.w0 & 15u, q1 = (ro.w0 >> 4) & 15u, q2 = (ro.w0 >> 8) & 15u;
+      const uint32_t dk = (ro.w0 >> 12) & 15u, dq = ro.w0 >> 16;
+      const uint32_t crm = ro.w1 & 0xFFu, ctm = (ro.w1 >> 8) & 0xFFFFu, perm = ro.w1 >> 24;
+      const uint32_t M = ro.w2;
+      const bool guard = ctm != 0;
+      if (guard) o << "      if ((tid & " << ctm << "u) == " << ctm << "u) {\n";
+      else o << "      {\n";
+      auto V = [&](int j) { return std::string("v") + std::to_string(var[j]); };
+      if (kind == RK_DENSE1) {
+        o << "        const " << T << " m00 = smat[" << M << "], m01 = smat[" << M + 1 << "], m10 = smat[" << M + 2
+          << "], m11 = smat[" << M + 3 << "];\n";
+        for (int j = 0; j < nr; ++j) {
+          if ((j >> q1) & 1) continue;
+          if ((static_cast<uint32_t>(j) & crm) != crm) continue;
+          const int k = j | (1 << q1);
+          o << "        { const " << T << " x = " << V(j) << ", y = " << V(k) << "; " << V(j)
+            << " = cfma(m01, y, cmul(m00, x)); " << V(k) << " = cfma(m11, y, cmul(m10, x)); }\n";
+        }
+      } else if (kind == RK_PERM1) {
+        for (int j = 0; j < nr; ++j) {
+          if ((j >> q1) & 1) continue;
+          if ((static_cast<uint32_t>(j) & crm) != crm) continue;
+          const int k = j | (1 << q1);
+          if (!guard) {
+            std::swap(var[j], var[k]);  // free: a rename
+          } else {
+            o << "        { const " << T << " x = " << V(j) << "; " << V(j) << " = " << V(k) << "; " << V(k)
+              << " = x; }\n";
+          }
+        }
+      } else if (kind == RK_DIAG) {
+        for (int j = 0; j < nr; ++j) {
+          if ((static_cast<uint32_t>(j) & crm) != crm) continue;
+          int idx = 0;
+          for (uint32_t i = 0; i < dk; ++i) idx = (idx << 1) | ((j >> ((dq >> (3 * i)) & 7u)) & 1);
+          o << "        " << V(j) << " = cmul(smat[" << M + idx << "], " << V(j) << ");\n";
+        }
+      } else if (kind == RK_DENSE2) {
+        o << "        " << T << " mm[16];\n        for (int e = 0; e < 16; ++e) mm[e] = smat[" << M << " + e];\n";
+        for (int j = 0; j < nr; ++j) {
+          if (((j >> q1) & 1) || ((j >> q2) & 1)) continue;
+          if ((static_cast<uint32_t>(j) & crm) != crm) continue;
+          const int id[4] = {j, j | (1 << q2), j | (1 << q1), j | (1 << q1) | (1 << q2)};
+          o << "        { const " << T << " a0 = " << V(id[0]) << ", a1 = " << V(id[1]) << ", a2 = " << V(id[2])
+            << ", a3 = " << V(id[3]) << ";\n";
+          for (int r = 0; r < 4; ++r)
+            o << "          " << V(id[r]) << " = cfma(mm[" << 4 * r + 3 << "], a3, cfma(mm[" << 4 * r + 2
+              << "], a2, cfma(mm[" << 4 * r + 1 << "], a1, cmul(mm[" << 4 * r << "], a0))));\n";
+          o << "        }\n";
+        }
+      } else {  // RK_PERM2: output row r takes input column p[r]
+        for (int j = 0; j < nr; ++j) {
+          if (((j >> q1) & 1) || ((j >> q2) & 1)) continue;
+          if ((static_cast<uint32_t>(j) & crm) != crm) continue;
+          const int id[4] = {j, j | (1 << q2), j | (1 << q1), j | (1 << q1) | (1 << q2)};
+          int pv[4];
+          for (int r = 0; r < 4; ++r) pv[r] = (perm >> (2 * r)) & 3u;
+          if (!guard) {
+            int nv[4];
+            for (int r = 0; r < 4; ++r) nv[r] = var[id[pv[r]]];
+            for (int r = 0; r < 4; ++r) var[id[r]] = nv[r];
+          } else {
+            o << "        { const " << T << " a0 = " << V(id[0]) << ", a1 = " << V(id[1]) << ", a2 = " << V(id[2])
+              << ", a3 = " << V(id[3]) << ";";
+            for (int r = 0; r < 4; ++r) o << " " << V(id[r]) << " = a" << pv[r] << ";";
+            o << " }\n";
+          }
+        }
+      }
+      o << "      }\n";
+    }
+    for (int j = 0; j < nr; ++j) o << "      s[tb" << nstage << " ^ " << off[j] << "u] = v" << var[j] << ";\n";
+    o << "    }\n    __syncthreads();\n";
+    ++nstage;
+  }
+  o << "    " << (c64 ? "store8<4>" : "store16<2>") << "(s, g, tbl, " << t << ", " << c << ");\n";
+  o << "  }\n}\n";
+}
+
+}  // namespace
+
+bool jit_available() {
+  std::call_once(g_once, init_bindings);
+  return g_nvrtc.ok && g_drv.ok;
+}
+
+bool jit_pass_eligible(const Schedule& s, int p) {
+  const PassDesc& pd = s.passes[p];
+  if (pd.step_end == pd.step_begin) return false;
+  for (int si = pd.step_begin; si < pd.step_end; ++si)
+    if (s.steps[si].kind != 0) return false;
+  return true;
+}
+
+// Kernel text of every eligible pass; identical texts share one kernel.
+void emit_all(const jq_plan* plan, const Schedule& s, std::string* src, std::vector<int>* kernel_of,
+              std::vector<std::string>* names) {
+  std::ostringstream all;
+  all << kPrelude;
+  kernel_of->assign(s.passes.size(), -1);
+  std::vector<std::string> texts;
+  for (int p = 0; p < static_cast<int>(s.passes.size()); ++p) {
+    if (!jit_pass_eligible(s, p)) continue;
+    std::ostringstream o;
+    emit_pass(o, plan, s, p, plan->dtype == JQ_C64, s.reg_bits);
+    const std::string text = o.str();
+    int k = -1;
+    for (size_t i = 0; i < texts.size(); ++i)
+      if (texts[i] == text) { k = static_cast<int>(i); break; }
+    if (k < 0) {
+      k = static_cast<int>(texts.size());
+      texts.push_back(text);
+      const std::string name = "jqk" + std::to_string(k);
+      names->push_back(name);
+      std::string body = text;
+      body.replace(body.find("@KERNEL@"), 8, name);
+      all << body;
+    }
+    (*kernel_of)[p] = k;
+  }
+  *src = all.str();
+}
+
+std::string jit_source(const jq_plan* plan, const Schedule& s) {
+  std::string src;
+  std::vector<int> kernel_of;
+  std::vector<std::string> names;
+  emit_all(plan, s, &src, &kernel_of, &names);
+  return src;
+}
+
+int jit_build(const jq_plan* plan, const Schedule& s, JitModule* out) {
+  if (!jit_available()) {
+    set_error("NVRTC or the CUDA driver entry points are not available");
+    return JQ_EUNSUPPORTED;
+  }
+  std::string src;
+  std::vector<int> kernel_of;
+  std::vector<std::string> names;
+  emit_all(plan, s, &src, &kernel_of, &names);
+  out->fn.assign(s.passes.size(), nullptr);
+  out->module = nullptr;
+  out->mc = nullptr;
+  out->mc_off.assign(s.passes.size(), 0);
+  if (names.empty()) return JQ_OK;
+  nvrtcProgram prog;
+  if (g_nvrtc.create(&prog, src.c_str(), "jq_plan.cu", 0, nullptr, nullptr) != NVRTC_SUCCESS) {
+    set_error("nvrtcCreateProgram failed");
+    return JQ_EUNSUPPORTED;
+  }
+  const char* opts[] = {"--gpu-architecture=sm_100a", "--std=c++17", "-default-device"};
+  const nvrtcResult cr = g_nvrtc.compile(prog, 3, opts);
+  if (cr != NVRTC_SUCCESS) {
+    size_t n = 0;
+    g_nvrtc.log_size(prog, &n);
+    std::string log(n, '\0');
+    g_nvrtc.log(prog, &log[0]);
+    g_nvrtc.destroy(&prog);
+    set_error("NVRTC compile of the plan failed: " + log.substr(0, 2000));
+    return JQ_EUNSUPPORTED;
+  }
+  size_t nbin = 0;
+  g_nvrtc.cubin_size(prog, &nbin);
+  std::vector<char> bin(nbin);
+  g_nvrtc.cubin(prog, bin.data());
+  g_nvrtc.destroy(&prog);
+  CUmodule mod;
+  if (g_drv.module_load(&mod, bin.data()) != CUDA_SUCCESS) {
+    set_error("cuModuleLoadData failed for the specialised plan");
+    return JQ_ECUDA;
+  }
+  out->module = mod;
+  std::vector<void*> fk(names.size(), nullptr);
+  for (size_t k = 0; k < names.size(); ++k) {
+    CUfunction f;
+    if (g_drv.get_function(&f, mod, names[k].c_str()) != CUDA_SUCCESS) {
+      set_error("cuModuleGetFunction failed for " + names[k]);
+      return JQ_ECUDA;
+    }
+    g_drv.set_attr(f, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, 227 * 1024);
+    fk[k] = f;
+  }
+  // per-pass matrix staging tables
+  std::vector<int32_t> mc;
+  for (int p = 0; p < static_cast<int>(s.passes.size()); ++p) {
+    if (kernel_of[p] < 0) continue;
+    out->fn[p] = fk[kernel_of[p]];
+    out->mc_off[p] = static_cast<int64_t>(mc.size());
+    const PassDesc& pd = s.passes[p];
+    for (int ri = pd.rop_begin; ri < pd.rop_end; ++ri) {
+      const RegOp& ro = s.rops[ri];
+      if (ro.mat_len <= 0) continue;
+      mc.push_back(static_cast<int32_t>(ro.w2));
+      mc.push_back(static_cast<int32_t>(ro.w3));
+      mc.push_back(ro.mat_len);
+    }
+  }
+  if (mc.empty()) mc.push_back(0);
+  if (cudaMalloc(&out->mc, mc.size() * sizeof(int32_t)) != cudaSuccess ||
+      cudaMemcpy(out->mc, mc.data(), mc.size() * sizeof(int32_t), cudaMemcpyHostToDevice) != cudaSuccess) {
+    set_error("upload of the matrix staging tables failed");
+    return JQ_ECUDA;
+  }
+  out->n_kernels = static_cast<int>(names.size());
+  return JQ_OK;
+}
+
+void jit_free(JitModule* m) {
+  if (m && m->module && g_drv.ok) g_drv.module_unload(static_cast<CUmodule>(m->module));
+  if (m && m->mc) cudaFree(m->mc);
+  if (m) {
+    m->mc = nullptr;
+    m->module = nullptr;
+    m->fn.clear();
+  }
+}
+
+size_t jit_smem(const Schedule& s, int p, int elem) {
+  const PassDesc& pd = s.passes[p];
+  return (static_cast<size_t>(1) << pd.t) * elem + static_cast<size_t>((pd.smat_len + 1) & ~1) * elem +
+         (static_cast<size_t>(1) << (pd.t - pd.c)) * 4;
+}
+
+int jit_launch(const JitModule& m, const Schedule& s, int p, int n_bits, int sm_count, void* state, int batch,
+               const void* bmat, int64_t bstride, int elem, cudaStream_t st) {
+  CUfunction f = static_cast<CUfunction>(m.fn[p]);
+  const PassDesc& pd = s.passes[p];
+  const int threads = 1 << (pd.t - s.reg_bits);
+  const size_t smem = jit_smem(s, p, elem);
+  int per_sm = 0;
+  g_drv.occupancy(&per_sm, f, threads, smem);
+  if (per_sm < 1) per_sm = 1;
+  const int64_t ntiles = (1LL << (n_bits - pd.t)) * batch;
+  const int64_t cap = static_cast<int64_t>(sm_count) * per_sm;
+  const unsigned grid = static_cast<unsigned>(std::max<int64_t>(1, std::min(ntiles, cap)));
+  long long bs = bstride;
+  const int32_t* mc = static_cast<const int32_t*>(m.mc) + m.mc_off[p];
+  void* args[] = {&state, &batch, const_cast<void**>(&bmat), &bs, &mc};
+  if (g_drv.launch(f, grid, 1, 1, threads, 1, 1, static_cast<unsigned>(smem), reinterpret_cast<CUstream>(st), args,
+                   nullptr) != CUDA_SUCCESS) {
+    set_error("cuLaunchKernel failed for a specialised pass");
+    return JQ_ECUDA;
+  }
+  return JQ_OK;
+}
+
+}  // namespace jq

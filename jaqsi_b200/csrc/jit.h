@@ -1,0 +1,30 @@
+// Per-plan specialised forward passes compiled with NVRTC (see jit.cpp).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "jq_internal.h"
+
+namespace jq {
+
+struct JitModule {
+  void* module = nullptr;       // CUmodule
+  std::vector<void*> fn;        // CUfunction per pass (nullptr: interpreter)
+  void* mc = nullptr;           // device int32 matrix staging tables
+  std::vector<int64_t> mc_off;  // per pass offset into mc
+  int n_kernels = 0;            // distinct kernels after sharing identical passes
+};
+
+bool jit_available();
+std::string jit_source(const jq_plan* plan, const Schedule& s);
+bool jit_pass_eligible(const Schedule& s, int p);
+int jit_build(const jq_plan* plan, const Schedule& s, JitModule* out);
+void jit_free(JitModule* m);
+size_t jit_smem(const Schedule& s, int p, int elem);
+int jit_launch(const JitModule& m, const Schedule& s, int p, int n_bits, int sm_count, void* state, int batch,
+               const void* bmat, int64_t bstride, int elem, cudaStream_t st);
+
+}  // namespace jq

@@ -74,8 +74,8 @@ struct TileOp {
   int32_t kt;          // target bits
   int32_t nfix;        // target + control bits
   uint32_t ctrl_mask;  // tile-local mask of the control bits (all must be 1)
-  int8_t fix[kMaxBlockWires];  // fixed bits, ascending
-  int8_t tb[kMaxBlockWires];   // target bits, tb[0] = most significant matrix bit
+  uint32_t lowmask[kMaxBlockWires];  // (1 << f) - 1 for each fixed bit f, ascending
+  uint32_t tmask[kMaxBlockWires];    // 1 << target bit; tmask[0] = most significant matrix bit
   int32_t mat_off, perm_off, grad_off;
 };
 
@@ -85,13 +85,49 @@ struct PassDesc {
   int32_t c;           // tile bits 0..c-1 are global bits 0..c-1
   uint64_t tile_mask;  // global bits held in the tile
   int32_t op_begin, op_end;
+  int32_t step_begin, step_end;  // register-stage program (empty: generic kernel)
+  int32_t rop_begin, rop_end;    // register ops of the program
+  int32_t smat_len;              // complex elements of the shared-memory matrix area
   int8_t bits[kMaxTileBits];  // global bit of each tile bit, ascending
+};
+
+// Register-stage program of a pass.  Each thread holds 2^r amplitudes of the
+// tile in registers (r "register bits" of the tile); a stage loads them from
+// shared memory, applies every op whose targets are register bits, and
+// stores them back.  Shared memory is XOR-swizzled (see swz_* in jqsim.cu);
+// ebits / tbits hold the swizzled offset of each register / thread bit.
+enum RegKind : int32_t { RK_DENSE1 = 0, RK_PERM1 = 1, RK_DIAG = 2, RK_DENSE2 = 3, RK_PERM2 = 4 };
+
+struct RegOp {
+  // w0: kind | q1 << 4 | q2 << 8 | dk << 12 | dq << 16 (dq: register bit of
+  //     DIAG target i at bits 3i..3i+2)
+  // w1: crm (control bits that are register bits, over j) | ctm << 8 (control
+  //     bits that are thread bits, over the thread index) | perm << 24
+  //     (PERM2 inner permutation, 2 bits per entry)
+  // w2: matrix offset in the pass's shared-memory matrix area
+  // w3: matrix offset in the block-matrix buffer (complex elements)
+  uint32_t w0, w1, w2, w3;
+  int32_t mat_len;     // complex elements of the matrix / diagonal (0: none)
+  int32_t pad[3];
+};
+
+constexpr int kMaxRegBits = 5;
+constexpr int kMaxThreadBits = kMaxTileBits - 4;
+
+struct Step {
+  int32_t kind;        // 0: register stage over rops[a, b); 1: generic shared-memory op tops[a]
+  int32_t a, b;
+  uint32_t ebits[kMaxRegBits];
+  uint32_t tbits[kMaxThreadBits];
 };
 
 struct Schedule {
   int32_t t = 0;
+  int32_t reg_bits = 0;  // r of the register-stage program (0: none)
   std::vector<PassDesc> passes;
   std::vector<TileOp> ops;
+  std::vector<Step> steps;
+  std::vector<RegOp> rops;
 };
 
 // Device copies of a plan's tables on one GPU.
@@ -103,10 +139,16 @@ struct DeviceTables {
   TileOp* fwd_ops = nullptr;
   TileOp* adj_ops = nullptr;
   TileOp* bwd_ops = nullptr;
+  Step* fwd_steps = nullptr;
+  RegOp* fwd_rops = nullptr;
+  Step* bwd_steps = nullptr;
+  RegOp* bwd_rops = nullptr;
   double* const_pool = nullptr;   // complex128 (re, im) pairs
   int32_t* perm_pool = nullptr;
   double* obs_pool = nullptr;     // dense observables, complex128
   void* obs_desc = nullptr;       // DevObs array
+  void* jit = nullptr;            // JitModule of the forward schedule (or nullptr)
+  bool jit_tried = false;
 };
 
 struct DevObs {
@@ -143,5 +185,6 @@ struct jq_plan {
   int64_t scratch_stride = 0;  // complex128 elements per instance (k > 2 blocks)
   int threads = 512;
   int ckpt_stride = 0;
+  bool jit = false;             // specialise the forward passes with NVRTC
   std::vector<jq::DeviceTables> dev;  // per-device uploads
 };

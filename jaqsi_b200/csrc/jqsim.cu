@@ -18,6 +18,7 @@
 
 #include "jq_internal.h"
 #include "kernels.cuh"
+#include "jit.h"
 
 namespace jq {
 void set_error(const std::string& msg);
@@ -44,20 +45,36 @@ __device__ __forceinline__ uint64_t pdep64(uint64_t v, uint64_t mask) {
   return r;
 }
 
+// Tile index of group g: zeros inserted at the op's fixed bits (ascending),
+// control bits set.  Fully unrolled so the descriptor stays in registers.
 __device__ __forceinline__ int group_base(int g, const TileOp& op) {
-  int b = g;
-  for (int i = 0; i < op.nfix; ++i) {
-    const int p = op.fix[i];
-    b = ((b >> p) << (p + 1)) | (b & ((1 << p) - 1));
+  uint32_t b = static_cast<uint32_t>(g);
+#pragma unroll
+  for (int i = 0; i < kMaxBlockWires; ++i) {
+    if (i < op.nfix) {
+      const uint32_t lm = op.lowmask[i];
+      b = ((b & ~lm) << 1) | (b & lm);
+    }
   }
-  return b | static_cast<int>(op.ctrl_mask);
+  return static_cast<int>(b | op.ctrl_mask);
 }
 
+// Tile offset of target combination j (bit kt-1-i of j <-> target i).
 __device__ __forceinline__ int target_off(int j, const TileOp& op, int kt) {
-  int o = 0;
-  for (int i = 0; i < kt; ++i)
-    if ((j >> (kt - 1 - i)) & 1) o |= 1 << op.tb[i];
-  return o;
+  uint32_t o = 0;
+#pragma unroll
+  for (int i = 0; i < kMaxBlockWires; ++i)
+    if (i < kt && ((j >> (kt - 1 - i)) & 1)) o |= op.tmask[i];
+  return static_cast<int>(o);
+}
+
+// Matrix index of tile element l: its target bits (target 0 most significant).
+__device__ __forceinline__ int target_index(int l, const TileOp& op) {
+  int a = 0;
+#pragma unroll
+  for (int i = 0; i < kMaxBlockWires; ++i)
+    if (i < op.kt) a = (a << 1) | ((static_cast<uint32_t>(l) & op.tmask[i]) ? 1 : 0);
+  return a;
 }
 
 // Sum `nv` per-thread doubles over the CTA; thread v < nv receives total v.
@@ -112,7 +129,7 @@ __device__ void tile_dense(C* s, int t, const TileOp& op, const C* __restrict__ 
 
 // Blocks on 3..6 target bits (rare): dynamic loops, group held in local memory.
 template <typename C>
-__device__ void tile_dense_wide(C* s, int t, const TileOp& op, const C* __restrict__ M, bool dag) {
+__device__ __noinline__ void tile_dense_wide(C* s, int t, const TileOp& op, const C* __restrict__ M, bool dag) {
   const int kt = op.kt, D = 1 << kt;
   const int G = 1 << (t - op.nfix);
   for (int g = threadIdx.x; g < G; g += blockDim.x) {
@@ -132,14 +149,11 @@ __device__ void tile_dense_wide(C* s, int t, const TileOp& op, const C* __restri
 
 template <typename C>
 __device__ void tile_diag(C* s, int t, const TileOp& op, const C* __restrict__ Dg, bool dag) {
-  const int kt = op.kt, D = 1 << kt;
-  const int G = 1 << (t - op.nfix);
-  const int total = G * D;
-  for (int e = threadIdx.x; e < total; e += blockDim.x) {
-    const int g = e >> kt, j = e & (D - 1);
-    const int idx = group_base(g, op) + target_off(j, op, kt);
-    const C d = dag ? cconj(Dg[j]) : Dg[j];
-    s[idx] = cmul(d, s[idx]);
+  const uint32_t cm = op.ctrl_mask;
+  for (int l = threadIdx.x; l < (1 << t); l += blockDim.x) {
+    if ((static_cast<uint32_t>(l) & cm) != cm) continue;
+    const C d = dag ? cconj(Dg[target_index(l, op)]) : Dg[target_index(l, op)];
+    s[l] = cmul(d, s[l]);
   }
 }
 
@@ -169,7 +183,7 @@ __device__ void tile_perm(C* s, int t, const TileOp& op, const int* __restrict__
 }
 
 template <typename C>
-__device__ void tile_perm_wide(C* s, int t, const TileOp& op, const int* __restrict__ P, bool inv) {
+__device__ __noinline__ void tile_perm_wide(C* s, int t, const TileOp& op, const int* __restrict__ P, bool inv) {
   const int kt = op.kt, D = 1 << kt;
   const int G = 1 << (t - op.nfix);
   for (int g = threadIdx.x; g < G; g += blockDim.x) {
@@ -223,22 +237,72 @@ __device__ __forceinline__ void fill_table(uint32_t* tbl, const PassDesc& pd) {
   }
 }
 
+// Tile <-> HBM copies.  Each thread keeps kBatch 16-byte loads in flight
+// before writing shared memory, so an SM has tens of KB outstanding (a plain
+// element loop leaves one load per warp in flight and is latency-bound).
+constexpr int kBatch = 8;
+// In the register-stage kernel the copy batch shares registers with the
+// stage arrays: 4 vectors (complex64) / 2 (complex128) keep it spill-free.
+template <typename C> struct SwzBatch { static constexpr int v = sizeof(C) == 8 ? 4 : 2; };
+
 template <typename C>
 __device__ __forceinline__ void tile_load(C* s, const C* g, const uint32_t* tbl, int t, int c) {
+  constexpr int V = 16 / sizeof(C);  // amplitudes per 16-byte vector
   const int cm = (1 << c) - 1;
-  for (int l = threadIdx.x; l < (1 << t); l += blockDim.x) s[l] = g[tbl[l >> c] | (l & cm)];
+  if (c >= (V == 2 ? 1 : 0)) {
+    const int nv = (1 << t) / V;
+    for (int v0 = threadIdx.x; v0 < nv; v0 += kBatch * blockDim.x) {
+      float4 r[kBatch];
+#pragma unroll
+      for (int u = 0; u < kBatch; ++u) {
+        const int v = v0 + u * blockDim.x;
+        if (v < nv) {
+          const int l = v * V;
+          r[u] = __ldcs(reinterpret_cast<const float4*>(g + (tbl[l >> c] | (l & cm))));
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < kBatch; ++u) {
+        const int v = v0 + u * blockDim.x;
+        if (v < nv) reinterpret_cast<float4*>(s)[v] = r[u];
+      }
+    }
+  } else {
+    for (int l = threadIdx.x; l < (1 << t); l += blockDim.x) s[l] = g[tbl[l >> c] | (l & cm)];
+  }
 }
 template <typename C>
 __device__ __forceinline__ void tile_store(const C* s, C* g, const uint32_t* tbl, int t, int c) {
+  constexpr int V = 16 / sizeof(C);
   const int cm = (1 << c) - 1;
-  for (int l = threadIdx.x; l < (1 << t); l += blockDim.x) g[tbl[l >> c] | (l & cm)] = s[l];
+  if (c >= (V == 2 ? 1 : 0)) {
+    const int nv = (1 << t) / V;
+    for (int v0 = threadIdx.x; v0 < nv; v0 += kBatch * blockDim.x) {
+      float4 r[kBatch];
+#pragma unroll
+      for (int u = 0; u < kBatch; ++u) {
+        const int v = v0 + u * blockDim.x;
+        if (v < nv) r[u] = reinterpret_cast<const float4*>(s)[v];
+      }
+#pragma unroll
+      for (int u = 0; u < kBatch; ++u) {
+        const int v = v0 + u * blockDim.x;
+        if (v < nv) {
+          const int l = v * V;
+          __stcs(reinterpret_cast<float4*>(g + (tbl[l >> c] | (l & cm))), r[u]);
+        }
+      }
+    }
+  } else {
+    for (int l = threadIdx.x; l < (1 << t); l += blockDim.x) g[tbl[l >> c] | (l & cm)] = s[l];
+  }
 }
 
 // ---------------------------------------------------------------------------
 // forward tile pass
 // ---------------------------------------------------------------------------
 template <typename R>
-__global__ void __launch_bounds__(1024) k_tile_fwd(typename CplxT<R>::T* __restrict__ state, int nb, int batch,
+__global__ void __launch_bounds__(512, 2) k_tile_fwd(typename CplxT<R>::T* __restrict__ state, int nb, int batch,
                                                    PassDesc pd, const TileOp* __restrict__ ops,
                                                    const typename CplxT<R>::T* __restrict__ bmat, int64_t bmat_stride,
                                                    const int* __restrict__ perms) {
@@ -266,6 +330,401 @@ __global__ void __launch_bounds__(1024) k_tile_fwd(typename CplxT<R>::T* __restr
       __syncthreads();
     }
     tile_store(s, g, tbl, t, c);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// register-stage forward pass
+// ---------------------------------------------------------------------------
+// Shared-memory swizzle: the bank bits of element l are XORed with all its
+// higher bits folded onto them (4 bank bits of 8-byte elements for complex64,
+// 3 of 16-byte elements for complex128).  Linear over XOR, so a tile offset
+// splits into per-bit offsets (Step::ebits / tbits).
+template <typename C> __device__ __forceinline__ uint32_t swz(uint32_t l);
+template <> __device__ __forceinline__ uint32_t swz<float2>(uint32_t l) {
+  return l ^ (((l >> 4) ^ (l >> 8) ^ (l >> 12)) & 15u);
+}
+template <> __device__ __forceinline__ uint32_t swz<double2>(uint32_t l) {
+  return l ^ (((l >> 3) ^ (l >> 6) ^ (l >> 9) ^ (l >> 12)) & 7u);
+}
+
+template <typename C>
+__device__ __forceinline__ void tile_load_swz(C* s, const C* g, const uint32_t* tbl, int t, int c) {
+  constexpr int V = 16 / sizeof(C);
+  const int cm = (1 << c) - 1;
+  const int nv = (1 << t) / V;
+  for (int v0 = threadIdx.x; v0 < nv; v0 += SwzBatch<C>::v * blockDim.x) {
+    float4 r[SwzBatch<C>::v];
+#pragma unroll
+    for (int u = 0; u < SwzBatch<C>::v; ++u) {
+      const int v = v0 + u * blockDim.x;
+      if (v < nv) {
+        const int l = v * V;
+        r[u] = __ldcs(reinterpret_cast<const float4*>(g + (tbl[l >> c] | (l & cm))));
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < SwzBatch<C>::v; ++u) {
+      const int v = v0 + u * blockDim.x;
+      if (v < nv) {
+        const uint32_t l = static_cast<uint32_t>(v * V);
+        if constexpr (V == 2) {
+          reinterpret_cast<float2*>(s)[swz<C>(l)] = make_float2(r[u].x, r[u].y);
+          reinterpret_cast<float2*>(s)[swz<C>(l + 1)] = make_float2(r[u].z, r[u].w);
+        } else {
+          reinterpret_cast<float4*>(s)[swz<C>(l)] = r[u];
+        }
+      }
+    }
+  }
+}
+
+template <typename C>
+__device__ __forceinline__ void tile_store_swz(const C* s, C* g, const uint32_t* tbl, int t, int c) {
+  constexpr int V = 16 / sizeof(C);
+  const int cm = (1 << c) - 1;
+  const int nv = (1 << t) / V;
+  for (int v0 = threadIdx.x; v0 < nv; v0 += SwzBatch<C>::v * blockDim.x) {
+    float4 r[SwzBatch<C>::v];
+#pragma unroll
+    for (int u = 0; u < SwzBatch<C>::v; ++u) {
+      const int v = v0 + u * blockDim.x;
+      if (v < nv) {
+        const uint32_t l = static_cast<uint32_t>(v * V);
+        if constexpr (V == 2) {
+          const float2 a = reinterpret_cast<const float2*>(s)[swz<C>(l)];
+          const float2 b = reinterpret_cast<const float2*>(s)[swz<C>(l + 1)];
+          r[u] = make_float4(a.x, a.y, b.x, b.y);
+        } else {
+          r[u] = reinterpret_cast<const float4*>(s)[swz<C>(l)];
+        }
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < SwzBatch<C>::v; ++u) {
+      const int v = v0 + u * blockDim.x;
+      if (v < nv) {
+        const int l = v * V;
+        __stcs(reinterpret_cast<float4*>(g + (tbl[l >> c] | (l & cm))), r[u]);
+      }
+    }
+  }
+}
+
+// Generic shared-memory op on the swizzled tile (blocks the register forms do
+// not cover): a copy of the group loop with swizzled addressing.
+template <typename C>
+__device__ __noinline__ void swz_apply_generic(C* s, int t, const TileOp& op, const C* __restrict__ bm,
+                                               const int* __restrict__ perms) {
+  const int kt = op.kt, D = 1 << kt;
+  const int G = 1 << (t - op.nfix);
+  for (int g = threadIdx.x; g < G; g += blockDim.x) {
+    const int base = group_base(g, op);
+    C v[64];
+#pragma unroll 1
+    for (int j = 0; j < D; ++j) v[j] = s[swz<C>(base + target_off(j, op, kt))];
+    if (op.kind == BK_DENSE) {
+      const C* M = bm + op.mat_off;
+#pragma unroll 1
+      for (int i = 0; i < D; ++i) {
+        C acc = cmake<C>(0, 0);
+#pragma unroll 1
+        for (int j = 0; j < D; ++j) acc = cfma(M[i * D + j], v[j], acc);
+        s[swz<C>(base + target_off(i, op, kt))] = acc;
+      }
+    } else if (op.kind == BK_DIAG) {
+      const C* Dg = bm + op.mat_off;
+#pragma unroll 1
+      for (int j = 0; j < D; ++j) s[swz<C>(base + target_off(j, op, kt))] = cmul(Dg[j], v[j]);
+    } else {
+      const int* P = perms + op.perm_off;
+#pragma unroll 1
+      for (int i = 0; i < D; ++i) s[swz<C>(base + target_off(i, op, kt))] = v[P[i]];
+    }
+  }
+}
+
+// --- register forms (NR amplitudes per thread, compile-time indices) --------
+// Controls that are register bits (crm) select per amplitude group with a
+// predicate-free select; CTRL = false is the common uncontrolled path.
+template <typename C>
+__device__ __forceinline__ C csel(bool p, const C& a, const C& b) {
+  C r;
+  r.x = p ? a.x : b.x;
+  r.y = p ? a.y : b.y;
+  return r;
+}
+
+template <typename C, int NR, int Q, bool CTRL>
+__device__ __forceinline__ void r_dense1(C (&a)[NR], const C* __restrict__ M, uint32_t crm) {
+  const C m00 = M[0], m01 = M[1], m10 = M[2], m11 = M[3];
+#pragma unroll
+  for (int j = 0; j < NR; ++j) {
+    if ((j >> Q) & 1) continue;
+    const int k = j | (1 << Q);
+    const C x = a[j], y = a[k];
+    const C nx = cfma(m01, y, cmul(m00, x));
+    const C ny = cfma(m11, y, cmul(m10, x));
+    if (CTRL) {
+      const bool on = (static_cast<uint32_t>(j) & crm) == crm;
+      a[j] = csel(on, nx, x);
+      a[k] = csel(on, ny, y);
+    } else {
+      a[j] = nx;
+      a[k] = ny;
+    }
+  }
+}
+
+// X on register bit Q, controlled by register bit QC: a pure register rename.
+template <typename C, int NR, int Q, int QC>
+__device__ __forceinline__ void r_cx(C (&a)[NR]) {
+#pragma unroll
+  for (int j = 0; j < NR; ++j) {
+    if (((j >> Q) & 1) || !((j >> QC) & 1)) continue;
+    const int k = j | (1 << Q);
+    const C x = a[j];
+    a[j] = a[k];
+    a[k] = x;
+  }
+}
+
+template <typename C, int NR, int Q>
+__device__ __forceinline__ void r_perm1(C (&a)[NR], uint32_t crm) {
+#pragma unroll
+  for (int j = 0; j < NR; ++j) {
+    if ((j >> Q) & 1) continue;
+    const int k = j | (1 << Q);
+    const bool on = (static_cast<uint32_t>(j) & crm) == crm;
+    const C x = a[j], y = a[k];
+    a[j] = csel(on, y, x);
+    a[k] = csel(on, x, y);
+  }
+}
+
+template <typename C, int NR, int Q1, int Q2>
+__device__ __forceinline__ void r_dense2(C (&a)[NR], const C* __restrict__ M, uint32_t crm) {
+#pragma unroll
+  for (int j = 0; j < NR; ++j) {
+    if (((j >> Q1) & 1) || ((j >> Q2) & 1)) continue;
+    const int i1 = j | (1 << Q2), i2 = j | (1 << Q1), i3 = j | (1 << Q1) | (1 << Q2);
+    const C v0 = a[j], v1 = a[i1], v2 = a[i2], v3 = a[i3];
+    const bool on = (static_cast<uint32_t>(j) & crm) == crm;
+    C o[4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+      o[r] = cfma(M[4 * r + 3], v3, cfma(M[4 * r + 2], v2, cfma(M[4 * r + 1], v1, cmul(M[4 * r], v0))));
+    a[j] = csel(on, o[0], v0);
+    a[i1] = csel(on, o[1], v1);
+    a[i2] = csel(on, o[2], v2);
+    a[i3] = csel(on, o[3], v3);
+  }
+}
+
+template <typename C>
+__device__ __forceinline__ C sel4(const C& v0, const C& v1, const C& v2, const C& v3, uint32_t i) {
+  return i == 0 ? v0 : i == 1 ? v1 : i == 2 ? v2 : v3;
+}
+
+template <typename C, int NR, int Q1, int Q2>
+__device__ __forceinline__ void r_perm2(C (&a)[NR], uint32_t perm, uint32_t crm) {
+#pragma unroll
+  for (int j = 0; j < NR; ++j) {
+    if (((j >> Q1) & 1) || ((j >> Q2) & 1)) continue;
+    const int i1 = j | (1 << Q2), i2 = j | (1 << Q1), i3 = j | (1 << Q1) | (1 << Q2);
+    const C v0 = a[j], v1 = a[i1], v2 = a[i2], v3 = a[i3];
+    const bool on = (static_cast<uint32_t>(j) & crm) == crm;
+    const uint32_t p = on ? perm : 0xE4u;  // 0xE4 = identity (0,1,2,3)
+    a[j] = sel4(v0, v1, v2, v3, p & 3u);
+    a[i1] = sel4(v0, v1, v2, v3, (p >> 2) & 3u);
+    a[i2] = sel4(v0, v1, v2, v3, (p >> 4) & 3u);
+    a[i3] = sel4(v0, v1, v2, v3, (p >> 6) & 3u);
+  }
+}
+
+template <typename C, int NR>
+__device__ __forceinline__ void r_diag(C (&a)[NR], const C* __restrict__ Dg, uint32_t dq, int dk, uint32_t crm) {
+#pragma unroll
+  for (int j = 0; j < NR; ++j) {
+    int idx = 0;
+#pragma unroll
+    for (int i = 0; i < kMaxRegBits; ++i)
+      if (i < dk) idx = (idx << 1) | ((j >> ((dq >> (3 * i)) & 7u)) & 1);
+    const bool on = (static_cast<uint32_t>(j) & crm) == crm;
+    a[j] = csel(on, cmul(Dg[idx], a[j]), a[j]);
+  }
+}
+
+#define JQ_Q1(F, ...)                                             \
+  switch (q1) {                                                   \
+    case 0: F<C, NR, 0 __VA_OPT__(,) __VA_ARGS__); break;         \
+    default: break;                                               \
+  }
+
+#define JQ_PAIR(F, A, B, ...) case (A) * 8 + (B): F<C, NR, A, B>(a __VA_OPT__(,) __VA_ARGS__); break;
+#define JQ_Q2(F, ...)                                                                                    \
+  switch (q1 * 8 + q2) {                                                                                 \
+    JQ_PAIR(F, 0, 1, __VA_ARGS__) JQ_PAIR(F, 0, 2, __VA_ARGS__) JQ_PAIR(F, 0, 3, __VA_ARGS__)             \
+    JQ_PAIR(F, 1, 0, __VA_ARGS__) JQ_PAIR(F, 1, 2, __VA_ARGS__) JQ_PAIR(F, 1, 3, __VA_ARGS__)             \
+    JQ_PAIR(F, 2, 0, __VA_ARGS__) JQ_PAIR(F, 2, 1, __VA_ARGS__) JQ_PAIR(F, 2, 3, __VA_ARGS__)             \
+    JQ_PAIR(F, 3, 0, __VA_ARGS__) JQ_PAIR(F, 3, 1, __VA_ARGS__) JQ_PAIR(F, 3, 2, __VA_ARGS__)             \
+    default:                                                                                              \
+      if constexpr (NR > 16) {                                                                            \
+        switch (q1 * 8 + q2) {                                                                            \
+          JQ_PAIR(F, 0, 4, __VA_ARGS__) JQ_PAIR(F, 1, 4, __VA_ARGS__) JQ_PAIR(F, 2, 4, __VA_ARGS__)       \
+          JQ_PAIR(F, 3, 4, __VA_ARGS__) JQ_PAIR(F, 4, 0, __VA_ARGS__) JQ_PAIR(F, 4, 1, __VA_ARGS__)       \
+          JQ_PAIR(F, 4, 2, __VA_ARGS__) JQ_PAIR(F, 4, 3, __VA_ARGS__)                                     \
+          default: break;                                                                                 \
+        }                                                                                                 \
+      }                                                                                                   \
+      break;                                                                                              \
+  }
+
+template <typename C, int NR, int Q>
+__device__ __forceinline__ void r_dense1_any(C (&a)[NR], const C* M, uint32_t crm) {
+  if (crm == 0) r_dense1<C, NR, Q, false>(a, M, 0);
+  else r_dense1<C, NR, Q, true>(a, M, crm);
+}
+
+template <typename C, int NR>
+__device__ __forceinline__ void reg_apply(C (&a)[NR], uint32_t w0, uint32_t w1, const C* M) {
+  const uint32_t ctm = (w1 >> 8) & 0xFFFFu;
+  if ((threadIdx.x & ctm) != ctm) return;
+  const uint32_t crm = w1 & 0xFFu;
+  const int q1 = (w0 >> 4) & 15, q2 = (w0 >> 8) & 15;
+  switch (w0 & 15u) {
+    case RK_DENSE1:
+      switch (q1) {
+        case 0: r_dense1_any<C, NR, 0>(a, M, crm); break;
+        case 1: r_dense1_any<C, NR, 1>(a, M, crm); break;
+        case 2: r_dense1_any<C, NR, 2>(a, M, crm); break;
+        case 3: r_dense1_any<C, NR, 3>(a, M, crm); break;
+        default: if constexpr (NR > 16) r_dense1_any<C, NR, (NR > 16 ? 4 : 0)>(a, M, crm); break;
+      }
+      break;
+    case RK_PERM1:
+      if (crm != 0 && (crm & (crm - 1)) == 0) {
+        // single control in a register bit: compile-time rename
+        switch (q1 * 8 + (__ffs(crm) - 1)) {
+          JQ_PAIR(r_cx, 0, 1) JQ_PAIR(r_cx, 0, 2) JQ_PAIR(r_cx, 0, 3)
+          JQ_PAIR(r_cx, 1, 0) JQ_PAIR(r_cx, 1, 2) JQ_PAIR(r_cx, 1, 3)
+          JQ_PAIR(r_cx, 2, 0) JQ_PAIR(r_cx, 2, 1) JQ_PAIR(r_cx, 2, 3)
+          JQ_PAIR(r_cx, 3, 0) JQ_PAIR(r_cx, 3, 1) JQ_PAIR(r_cx, 3, 2)
+          default:
+            if constexpr (NR > 16) {
+              switch (q1 * 8 + (__ffs(crm) - 1)) {
+                JQ_PAIR(r_cx, 0, 4) JQ_PAIR(r_cx, 1, 4) JQ_PAIR(r_cx, 2, 4) JQ_PAIR(r_cx, 3, 4)
+                JQ_PAIR(r_cx, 4, 0) JQ_PAIR(r_cx, 4, 1) JQ_PAIR(r_cx, 4, 2) JQ_PAIR(r_cx, 4, 3)
+                default: break;
+              }
+            }
+            break;
+        }
+        break;
+      }
+      switch (q1) {
+        case 0: r_perm1<C, NR, 0>(a, crm); break;
+        case 1: r_perm1<C, NR, 1>(a, crm); break;
+        case 2: r_perm1<C, NR, 2>(a, crm); break;
+        case 3: r_perm1<C, NR, 3>(a, crm); break;
+        default: if constexpr (NR > 16) r_perm1<C, NR, (NR > 16 ? 4 : 0)>(a, crm); break;
+      }
+      break;
+    case RK_DIAG: r_diag<C, NR>(a, M, w0 >> 16, (w0 >> 12) & 15, crm); break;
+    case RK_DENSE2: JQ_Q2(r_dense2, M, crm) break;
+    default: JQ_Q2(r_perm2, w1 >> 24, crm) break;
+  }
+}
+
+constexpr int kStepWords = sizeof(Step) / 4;
+
+template <typename R, int RB>
+__global__ void __launch_bounds__(256, 2) k_tile_fwd2(typename CplxT<R>::T* __restrict__ state, int nb, int batch,
+                                                      PassDesc pd, const Step* __restrict__ steps,
+                                                      const RegOp* __restrict__ rops, const TileOp* __restrict__ tops,
+                                                      const typename CplxT<R>::T* __restrict__ bmat,
+                                                      int64_t bmat_stride, const int* __restrict__ perms) {
+  using C = typename CplxT<R>::T;
+  constexpr int NR = 1 << RB;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int t = pd.t, c = pd.c;
+  const int nst = pd.step_end - pd.step_begin, nro = pd.rop_end - pd.rop_begin;
+  C* s = reinterpret_cast<C*>(smem_raw);
+  C* smat = s + (1 << t);
+  uint32_t* tbl = reinterpret_cast<uint32_t*>(smat + ((pd.smat_len + 1) & ~1));
+  // every region starts on a 16-byte boundary (sro is read as uint4)
+  uint32_t* sst = tbl + (((1 << (t - c)) + 3) & ~3);
+  uint4* sro = reinterpret_cast<uint4*>(sst + ((nst * kStepWords + 3) & ~3));
+  fill_table(tbl, pd);
+  {
+    const uint32_t* src = reinterpret_cast<const uint32_t*>(steps + pd.step_begin);
+    for (int i = threadIdx.x; i < nst * kStepWords; i += blockDim.x) sst[i] = src[i];
+    for (int i = threadIdx.x; i < nro; i += blockDim.x) {
+      const RegOp ro = rops[pd.rop_begin + i];
+      sro[i] = make_uint4(ro.w0, ro.w1, ro.w2, ro.w3);
+    }
+  }
+  const int64_t tiles_per = 1LL << (nb - t);
+  const int64_t ntiles = tiles_per * batch;
+  const uint64_t full = (nb >= 64) ? ~0ULL : ((1ULL << nb) - 1);
+  const uint64_t outer_mask = full & ~pd.tile_mask;
+  const int nthr_bits = t - RB;
+  int64_t last_inst = -1;
+  for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int64_t inst = tile >> (nb - t);
+    const uint64_t ti = static_cast<uint64_t>(tile) & static_cast<uint64_t>(tiles_per - 1);
+    C* g = state + (inst << nb) + pdep64(ti, outer_mask);
+    const C* bm = bmat + inst * bmat_stride;
+    __syncthreads();
+    if (inst != last_inst) {
+      // gate matrices of this pass for this instance
+      for (int i = 0; i < nro; ++i) {
+        const RegOp& ro = rops[pd.rop_begin + i];
+        for (int e = threadIdx.x; e < ro.mat_len; e += blockDim.x) smat[ro.w2 + e] = bm[ro.w3 + e];
+      }
+      last_inst = inst;
+    }
+    tile_load_swz(s, g, tbl, t, c);
+    __syncthreads();
+    for (int si = 0; si < nst; ++si) {
+      const uint32_t* st = sst + si * kStepWords;
+      // Step layout: kind, a, b, ebits[kMaxRegBits], tbits[kMaxThreadBits]
+      if (st[0] == 1u) {
+        swz_apply_generic<C>(s, t, tops[st[1]], bm, perms);
+        __syncthreads();
+        continue;
+      }
+      uint32_t tb = 0;
+      for (int i = 0; i < nthr_bits; ++i)
+        if ((threadIdx.x >> i) & 1) tb ^= st[3 + kMaxRegBits + i];
+      uint32_t e[RB];
+#pragma unroll
+      for (int q = 0; q < RB; ++q) e[q] = st[3 + q];
+      C a[NR];
+#pragma unroll
+      for (int j = 0; j < NR; ++j) {
+        uint32_t o = tb;
+#pragma unroll
+        for (int q = 0; q < RB; ++q)
+          if ((j >> q) & 1) o ^= e[q];
+        a[j] = s[o];
+      }
+      const int ob = static_cast<int>(st[1]) - pd.rop_begin, oe = static_cast<int>(st[2]) - pd.rop_begin;
+      for (int oi = ob; oi < oe; ++oi) {
+        const uint4 ro = sro[oi];
+        reg_apply<C, NR>(a, ro.x, ro.y, smat + ro.z);
+      }
+#pragma unroll
+      for (int j = 0; j < NR; ++j) {
+        uint32_t o = tb;
+#pragma unroll
+        for (int q = 0; q < RB; ++q)
+          if ((j >> q) & 1) o ^= e[q];
+        s[o] = a[j];
+      }
+      __syncthreads();
+    }
+    tile_store_swz(s, g, tbl, t, c);
   }
 }
 
@@ -336,7 +795,7 @@ __device__ void adj_dense(C* sp, C* sl, int t, const TileOp& op, const C* __rest
 
 // Wide blocks (3..6 target bits): dynamic loops, gradient by direct atomics.
 template <typename C>
-__device__ void adj_dense_wide(C* sp, C* sl, int t, const TileOp& op, const C* __restrict__ M, double2* gacc) {
+__device__ __noinline__ void adj_dense_wide(C* sp, C* sl, int t, const TileOp& op, const C* __restrict__ M, double2* gacc) {
   const int kt = op.kt, D = 1 << kt;
   const int G = 1 << (t - op.nfix);
   const bool grad = op.grad_off >= 0;
@@ -434,7 +893,7 @@ __device__ void adj_apply(C* sp, C* sl, int t, const TileOp& op, const C* bm, co
 }
 
 template <typename R>
-__global__ void __launch_bounds__(1024) k_tile_adj(typename CplxT<R>::T* __restrict__ psi,
+__global__ void __launch_bounds__(512, 1) k_tile_adj(typename CplxT<R>::T* __restrict__ psi,
                                                    typename CplxT<R>::T* __restrict__ lam, int nb, int batch,
                                                    PassDesc pd, const TileOp* __restrict__ ops,
                                                    const typename CplxT<R>::T* __restrict__ bmat, int64_t bmat_stride,
@@ -528,7 +987,7 @@ __device__ void bwd_dense(const C* sx, C* sl, int t, const TileOp& op, const C* 
 }
 
 template <typename C>
-__device__ void bwd_dense_wide(const C* sx, C* sl, int t, const TileOp& op, const C* __restrict__ M,
+__device__ __noinline__ void bwd_dense_wide(const C* sx, C* sl, int t, const TileOp& op, const C* __restrict__ M,
                                double2* gacc) {
   const int kt = op.kt, D = 1 << kt;
   const int G = 1 << (t - op.nfix);
@@ -598,7 +1057,7 @@ __device__ void bwd_diag(const C* sx, C* sl, int t, const TileOp& op, const C* _
 }
 
 template <typename R>
-__global__ void __launch_bounds__(1024) k_tile_bwd(const typename CplxT<R>::T* __restrict__ x,
+__global__ void __launch_bounds__(512, 1) k_tile_bwd(const typename CplxT<R>::T* __restrict__ x,
                                                    typename CplxT<R>::T* __restrict__ lam, int nb, int batch,
                                                    PassDesc pd, const TileOp* __restrict__ ops,
                                                    const typename CplxT<R>::T* __restrict__ bmat, int64_t bmat_stride,
@@ -881,6 +1340,17 @@ template <typename R>
 __global__ void k_expval_pauli_sv(const typename CplxT<R>::T* psi, int64_t dim, const DevObs* obs, int o_begin,
                                   int o_cnt, double* out, int n_obs) {
   __shared__ double red[32 * kRedSlots];
+  __shared__ uint64_t sx[kObsChunk], sz[kObsChunk];
+  __shared__ double sc[kObsChunk];
+  __shared__ int sy[kObsChunk];
+  if (threadIdx.x < o_cnt) {
+    const DevObs ob = obs[o_begin + threadIdx.x];
+    sx[threadIdx.x] = ob.x_mask;
+    sz[threadIdx.x] = ob.z_mask;
+    sc[threadIdx.x] = ob.coeff;
+    sy[threadIdx.x] = ob.n_y;
+  }
+  __syncthreads();
   const int inst = blockIdx.y;
   const auto* p = psi + static_cast<int64_t>(inst) * dim;
   double acc[kObsChunk];
@@ -889,19 +1359,19 @@ __global__ void k_expval_pauli_sv(const typename CplxT<R>::T* psi, int64_t dim, 
   for (int64_t j = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < dim;
        j += static_cast<int64_t>(gridDim.x) * blockDim.x) {
     const double2 a = to_d2(p[j]);
+    const double pa = a.x * a.x + a.y * a.y;
 #pragma unroll
     for (int o = 0; o < kObsChunk; ++o) {
       if (o < o_cnt) {
-        const DevObs ob = obs[o_begin + o];
-        const int64_t jx = j ^ static_cast<int64_t>(ob.x_mask);
+        const uint64_t x = sx[o];
+        const int64_t jx = j ^ static_cast<int64_t>(x);
         // (P psi)_j = phase(j ^ x) psi_{j ^ x}
-        const double sign = (__popcll(static_cast<uint64_t>(jx) & ob.z_mask) & 1) ? -1.0 : 1.0;
-        if (ob.x_mask == 0) {
-          acc[o] += ob.coeff * sign * (a.x * a.x + a.y * a.y);
+        const double sign = (__popcll(static_cast<uint64_t>(jx) & sz[o]) & 1) ? -sc[o] : sc[o];
+        if (x == 0) {
+          acc[o] += sign * pa;
         } else {
-          const double2 bv = to_d2(p[jx]);
-          const double2 w = cmul(cconj(a), bv);
-          acc[o] += ob.coeff * sign * re_iy(ob.n_y, w);
+          const double2 w = cmul(cconj(a), to_d2(p[jx]));
+          acc[o] += sign * re_iy(sy[o], w);
         }
       }
     }
@@ -1222,6 +1692,19 @@ int device_tables(const jq_plan* cplan, const DeviceTables** out) {
   TileOp* bo = nullptr;
   if ((rc = upload(plan->bwd.ops, &bo))) return rc;
   t.bwd_ops = bo;
+  if ((rc = upload(plan->fwd.steps, &t.fwd_steps))) return rc;
+  if ((rc = upload(plan->fwd.rops, &t.fwd_rops))) return rc;
+  if ((rc = upload(plan->bwd.steps, &t.bwd_steps))) return rc;
+  if ((rc = upload(plan->bwd.rops, &t.bwd_rops))) return rc;
+  if (plan->jit && jit_available()) {
+    JitModule* jm = new JitModule();
+    if (jit_build(plan, plan->fwd, jm) == JQ_OK) {
+      t.jit = jm;
+    } else {
+      delete jm;  // the interpreter kernels run instead
+    }
+  }
+  t.jit_tried = true;
   plan->dev.push_back(t);
   *out = &plan->dev.back();
   return JQ_OK;
@@ -1293,6 +1776,8 @@ int set_smem_attrs() {
   JQ_CUDA(cudaFuncSetAttribute(k_tile_fwd<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem));
   JQ_CUDA(cudaFuncSetAttribute(k_tile_adj<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem));
   JQ_CUDA(cudaFuncSetAttribute(k_tile_bwd<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem));
+  JQ_CUDA(cudaFuncSetAttribute(k_tile_fwd2<R, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               max_smem));
   done = true;
   return JQ_OK;
 }
@@ -1306,19 +1791,41 @@ int ctas_for(K kernel, int threads, size_t smem, int64_t ntiles) {
   return static_cast<int>(std::max<int64_t>(1, std::min(ntiles, cap)));
 }
 
-// Run passes [p0, p1) of a schedule over `state` (batch instances).
+// Run passes [p0, p1) of a schedule over `state` (batch instances).  Passes
+// with a register-stage program use k_tile_fwd2, the others k_tile_fwd.
 template <typename R>
-int run_passes(const jq_plan* plan, const Schedule& sch, const TileOp* dops, const DeviceTables* T,
-               typename CplxT<R>::T* state, int batch, const typename CplxT<R>::T* bmat, size_t p0, size_t p1,
-               cudaStream_t st) {
+int run_passes(const jq_plan* plan, const Schedule& sch, const TileOp* dops, const Step* dsteps,
+               const RegOp* drops, const DeviceTables* T, typename CplxT<R>::T* state, int batch,
+               const typename CplxT<R>::T* bmat, size_t p0, size_t p1, cudaStream_t st,
+               const JitModule* jm = nullptr) {
+  constexpr int RB = 4;
   for (size_t p = p0; p < p1; ++p) {
     const PassDesc& pd = sch.passes[p];
     if (pd.op_end == pd.op_begin) continue;
+    if (jm && p < jm->fn.size() && jm->fn[p]) {
+      const int rc = jit_launch(*jm, sch, static_cast<int>(p), plan->n_bits, sm_count(), state, batch, bmat,
+                                plan->bmat_stride, static_cast<int>(sizeof(typename CplxT<R>::T)), st);
+      if (rc) return rc;
+      continue;
+    }
     const size_t smem = tile_smem<R>(pd, 1);
     const int64_t ntiles = (1LL << (plan->n_bits - pd.t)) * batch;
-    const int ctas = ctas_for(k_tile_fwd<R>, plan->threads, smem, ntiles);
-    k_tile_fwd<R><<<ctas, plan->threads, smem, st>>>(state, plan->n_bits, batch, pd, dops, bmat, plan->bmat_stride,
-                                                      T->perm_pool);
+    if (pd.step_end > pd.step_begin) {
+      const int threads = 1 << (pd.t - RB);
+      const size_t elem = sizeof(typename CplxT<R>::T);
+      const int nst = pd.step_end - pd.step_begin;
+      const size_t smem2 = (static_cast<size_t>(1) << pd.t) * elem + ((pd.smat_len + 1) & ~1) * elem +
+                           (((static_cast<size_t>(1) << (pd.t - pd.c)) + 3) & ~static_cast<size_t>(3)) * 4 +
+                           ((nst * kStepWords + 3) & ~3) * 4 +
+                           static_cast<size_t>(pd.rop_end - pd.rop_begin) * 16;
+      const int ctas = ctas_for(k_tile_fwd2<R, RB>, threads, smem2, ntiles);
+      k_tile_fwd2<R, RB><<<ctas, threads, smem2, st>>>(state, plan->n_bits, batch, pd, dsteps, drops, dops, bmat,
+                                                       plan->bmat_stride, T->perm_pool);
+    } else {
+      const int ctas = ctas_for(k_tile_fwd<R>, plan->threads, smem, ntiles);
+      k_tile_fwd<R><<<ctas, plan->threads, smem, st>>>(state, plan->n_bits, batch, pd, dops, bmat, plan->bmat_stride,
+                                                        T->perm_pool);
+    }
   }
   JQ_CUDA(cudaGetLastError());
   return JQ_OK;
@@ -1419,8 +1926,30 @@ int forward_impl(const jq_plan* plan, int batch, const double* angles, const voi
   k_init<R><<<grid_for(plan->state_elems * batch, 256), 256, 0, st>>>(
       S, plan->state_elems, batch, static_cast<const C*>(init), dim, init_batched, dm && init ? 1 : 0);
   JQ_CUDA(cudaGetLastError());
-  if ((rc = run_passes<R>(plan, plan->fwd, T->fwd_ops, T, S, batch, bmat, 0, plan->fwd.passes.size(), st))) return rc;
+  if ((rc = run_passes<R>(plan, plan->fwd, T->fwd_ops, T->fwd_steps, T->fwd_rops, T, S, batch, bmat, 0, plan->fwd.passes.size(), st,
+                          static_cast<const JitModule*>(T->jit)))) return rc;
   return measure<R>(plan, T, batch, out_type, S, out, st);
+}
+
+template <typename R>
+int sweep_impl(const jq_plan* plan, int batch, const double* angles, const void* mats, void* state, void* ws,
+               size_t ws_bytes, cudaStream_t st) {
+  using C = typename CplxT<R>::T;
+  const DeviceTables* T = nullptr;
+  int rc = device_tables(plan, &T);
+  if (rc) return rc;
+  if ((rc = set_smem_attrs<R>())) return rc;
+  WsLayout L = layout(plan, batch, 0);
+  if (ws_bytes < L.total || (L.total > 0 && !ws)) {
+    set_error("workspace too small: need " + std::to_string(L.total) + " bytes");
+    return JQ_ENOMEM;
+  }
+  char* w = static_cast<char*>(ws);
+  C* bmat = reinterpret_cast<C*>(w + L.bmat);
+  double2* scratch = reinterpret_cast<double2*>(w + L.scratch);
+  if ((rc = prep<R>(plan, T, batch, angles, mats, bmat, scratch, st))) return rc;
+  return run_passes<R>(plan, plan->fwd, T->fwd_ops, T->fwd_steps, T->fwd_rops, T, static_cast<C*>(state), batch, bmat, 0,
+                       plan->fwd.passes.size(), st, static_cast<const JitModule*>(T->jit));
 }
 
 template <typename R>
@@ -1585,7 +2114,7 @@ int backward_impl(const jq_plan* plan, int batch, const double* angles, const vo
   const int64_t S = L.seg_len;
   for (int64_t p = 0; p < P; ++p) {
     if (p % S == 0) JQ_CUDA(cudaMemcpyAsync(ckpt(p / S), work, sizeof(C) * elems * batch, cudaMemcpyDeviceToDevice, st));
-    if ((rc = run_passes<R>(plan, sch, T->bwd_ops, T, work, batch, bmat, p, p + 1, st))) return rc;
+    if ((rc = run_passes<R>(plan, sch, T->bwd_ops, T->bwd_steps, T->bwd_rops, T, work, batch, bmat, p, p + 1, st))) return rc;
   }
   // seed
   if (dm) rc = seed_dm<R>(plan, T, batch, out_type, ct, ct_state, lam, st);
@@ -1599,7 +2128,7 @@ int backward_impl(const jq_plan* plan, int batch, const double* angles, const vo
     JQ_CUDA(cudaMemcpyAsync(seg(0), ckpt(c), sizeof(C) * elems * batch, cudaMemcpyDeviceToDevice, st));
     for (int64_t j = 0; j + 1 < p1 - p0; ++j) {
       JQ_CUDA(cudaMemcpyAsync(seg(j + 1), seg(j), sizeof(C) * elems * batch, cudaMemcpyDeviceToDevice, st));
-      if ((rc = run_passes<R>(plan, sch, T->bwd_ops, T, seg(j + 1), batch, bmat, p0 + j, p0 + j + 1, st))) return rc;
+      if ((rc = run_passes<R>(plan, sch, T->bwd_ops, T->bwd_steps, T->bwd_rops, T, seg(j + 1), batch, bmat, p0 + j, p0 + j + 1, st))) return rc;
     }
     for (int64_t p = p1 - 1; p >= p0; --p) {
       const PassDesc& pd = sch.passes[p];
@@ -1659,7 +2188,12 @@ int jq_plan_free(jq_plan* plan) {
   for (DeviceTables& t : plan->dev) {
     if (t.device >= 0) cudaSetDevice(t.device);
     cudaFree(t.ops); cudaFree(t.prims); cudaFree(t.blocks); cudaFree(t.fwd_ops); cudaFree(t.adj_ops);
-    cudaFree(t.bwd_ops); cudaFree(t.const_pool); cudaFree(t.perm_pool); cudaFree(t.obs_pool); cudaFree(t.obs_desc);
+    cudaFree(t.bwd_ops); cudaFree(t.fwd_steps); cudaFree(t.fwd_rops); cudaFree(t.bwd_steps); cudaFree(t.bwd_rops);
+    cudaFree(t.const_pool);
+    if (t.jit) {
+      jit_free(static_cast<JitModule*>(t.jit));
+      delete static_cast<JitModule*>(t.jit);
+    } cudaFree(t.perm_pool); cudaFree(t.obs_pool); cudaFree(t.obs_desc);
   }
   if (cur >= 0 && !plan->dev.empty()) cudaSetDevice(cur);
   delete plan;
@@ -1685,6 +2219,10 @@ int jq_plan_get_info(const jq_plan* plan, jq_plan_info* info) {
   info->n_obs = static_cast<int32_t>(plan->obs.size());
   info->unitary = plan->unitary ? 1 : 0;
   info->state_elems = plan->state_elems;
+  for (const Step& st : plan->fwd.steps) {
+    if (st.kind == 0) ++info->n_stages_fwd;
+    else ++info->n_smem_ops_fwd;
+  }
   return JQ_OK;
 }
 
@@ -1700,6 +2238,17 @@ int jq_plan_block_passes(const jq_plan* plan, int which, int32_t* block_pass, in
       for (int j = 0; j < kMaxBlockWires; ++j) block_wires[b * kMaxBlockWires + j] = plan->block_wires[b][j];
   }
   return JQ_OK;
+}
+
+size_t jq_plan_jit_source(const jq_plan* plan, char* buf, size_t n) {
+  if (!plan) return 0;
+  const std::string src = jit_source(plan, plan->fwd);
+  if (buf && n > 0) {
+    const size_t k = std::min(n - 1, src.size());
+    std::memcpy(buf, src.data(), k);
+    buf[k] = '\0';
+  }
+  return src.size();
 }
 
 size_t jq_workspace_bytes(const jq_plan* plan, int batch, int out_type, int with_grad) {
@@ -1736,6 +2285,16 @@ int jq_forward(const jq_plan* plan, int batch, const double* angles, const void*
                                workspace_bytes, st);
   return forward_impl<double>(plan, batch, angles, mats, init, init_batched, out_type, state, out, workspace,
                               workspace_bytes, st);
+}
+
+int jq_sweep(const jq_plan* plan, int batch, const double* angles, const void* mats, void* state, void* workspace,
+             size_t workspace_bytes, void* stream) {
+  int rc = check_common(plan, batch, angles, mats);
+  if (rc) return rc;
+  if (!state) { set_error("jq_sweep: state is NULL"); return JQ_EINVAL; }
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (plan->dtype == JQ_C64) return sweep_impl<float>(plan, batch, angles, mats, state, workspace, workspace_bytes, st);
+  return sweep_impl<double>(plan, batch, angles, mats, state, workspace, workspace_bytes, st);
 }
 
 int jq_adjoint(const jq_plan* plan, int batch, const double* angles, const void* mats, const void* state,

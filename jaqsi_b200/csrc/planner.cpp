@@ -16,6 +16,7 @@
 #include <cmath>
 #include <complex>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 #include <string>
@@ -205,10 +206,10 @@ Schedule schedule(const std::vector<HostBlock>& blocks, const std::vector<DevBlo
         int bit = nb - 1 - blocks[b].wires[i];
         pos[i] = rank[bit];
         if (i < db.n_ctrl) op.ctrl_mask |= 1u << pos[i];
-        else op.tb[i - db.n_ctrl] = static_cast<int8_t>(pos[i]);
+        else op.tmask[i - db.n_ctrl] = 1u << pos[i];
       }
       std::sort(pos, pos + db.k);
-      for (int i = 0; i < db.k; ++i) op.fix[i] = static_cast<int8_t>(pos[i]);
+      for (int i = 0; i < db.k; ++i) op.lowmask[i] = (1u << pos[i]) - 1u;
       op.mat_off = db.mat_off;
       op.perm_off = db.perm_off;
       op.grad_off = db.grad_off;
@@ -220,9 +221,157 @@ Schedule schedule(const std::vector<HostBlock>& blocks, const std::vector<DevBlo
   return s;
 }
 
+// Swizzled shared-memory offset of tile bit `pos` (linear over XOR): bank
+// bits are folded from all higher bits so that any 4 (c64) / 3 (c128) lane
+// bits with distinct residues hit distinct banks.
+uint32_t swz_bit(int pos, int dtype) {
+  const int nbank = (dtype == JQ_C64) ? 4 : 3;
+  uint32_t v = 1u << pos;
+  if (pos >= nbank) v |= 1u << (pos % nbank);
+  return v;
+}
+
+// Register-stage program of every pass of `s` (see Step in jq_internal.h).
+// Ops join the current stage greedily in program order while their targets
+// fit in r register bits; an op that does not fit, or that touches a bit of a
+// deferred op, is deferred to a later stage.  Ops with more targets than the
+// register forms cover run as generic shared-memory steps.
+void build_steps(Schedule& s, const std::vector<int32_t>& perm_pool, int dtype) {
+  const int r = 4;
+  s.reg_bits = r;
+  for (PassDesc& pd : s.passes) {
+    pd.step_begin = pd.step_end = static_cast<int32_t>(s.steps.size());
+    pd.rop_begin = pd.rop_end = static_cast<int32_t>(s.rops.size());
+    pd.smat_len = 0;
+    int smat = 0;
+    const int t = pd.t;
+    if (t < r + 5 || t > r + 8) continue;  // 32..256 threads per CTA, else generic kernel
+    std::vector<int> rem;
+    for (int o = pd.op_begin; o < pd.op_end; ++o) rem.push_back(o);
+    auto targets_of = [&](const TileOp& op) {
+      uint32_t m = 0;
+      for (int i = 0; i < op.kt; ++i) m |= op.tmask[i];
+      return m;
+    };
+    auto reg_ok = [&](const TileOp& op) {
+      if (op.kind == BK_DENSE) return op.kt <= 2;
+      if (op.kind == BK_DIAG) return op.kt <= r;
+      if (op.kind == BK_PERM) {
+        if (op.kt == 2) return true;
+        if (op.kt == 1) return perm_pool[op.perm_off] == 1 || perm_pool[op.perm_off] == 0;
+        return false;
+      }
+      return false;
+    };
+    while (!rem.empty()) {
+      uint32_t R = 0, blocked = 0;
+      std::vector<int> members;
+      int smem_op = -1;
+      for (int o : rem) {
+        const TileOp& op = s.ops[o];
+        const uint32_t tg = targets_of(op), all = tg | op.ctrl_mask;
+        if (all & blocked) { blocked |= all; continue; }
+        if (!reg_ok(op)) {
+          if (members.empty()) { smem_op = o; break; }
+          blocked |= all;
+          continue;
+        }
+        if (__builtin_popcount(R | tg) <= r) {
+          R |= tg;
+          members.push_back(o);
+        } else {
+          blocked |= all;
+        }
+      }
+      Step st;
+      std::memset(&st, 0, sizeof(st));
+      if (smem_op >= 0) {
+        st.kind = 1;
+        st.a = smem_op;
+        st.b = smem_op + 1;
+        s.steps.push_back(st);
+        rem.erase(std::find(rem.begin(), rem.end(), smem_op));
+        continue;
+      }
+      // fill the register set with the highest free tile bits (lanes then
+      // map to the lowest bits, which keeps shared memory conflict-free)
+      for (int pos = t - 1; pos >= 0 && __builtin_popcount(R) < r; --pos) R |= 1u << pos;
+      int rank_r[32], rank_t[32];
+      int nr = 0, nt = 0;
+      for (int pos = 0; pos < t; ++pos) {
+        if (R >> pos & 1u) {
+          st.ebits[nr] = swz_bit(pos, dtype);
+          rank_r[pos] = nr++;
+          rank_t[pos] = -1;
+        } else {
+          st.tbits[nt] = swz_bit(pos, dtype);
+          rank_t[pos] = nt++;
+          rank_r[pos] = -1;
+        }
+      }
+      st.kind = 0;
+      st.a = static_cast<int32_t>(s.rops.size());
+      for (int o : members) {
+        const TileOp& op = s.ops[o];
+        RegOp ro;
+        std::memset(&ro, 0, sizeof(ro));
+        auto qpos = [&](uint32_t mask) { return static_cast<uint32_t>(rank_r[__builtin_ctz(mask)]); };
+        uint32_t crm = 0, ctm = 0;
+        for (int pos = 0; pos < t; ++pos) {
+          if (!(op.ctrl_mask >> pos & 1u)) continue;
+          if (rank_r[pos] >= 0) crm |= 1u << rank_r[pos];
+          else ctm |= 1u << rank_t[pos];
+        }
+        uint32_t kind = 0, q1 = 0, q2 = 0, dk = 0, dq = 0, perm = 0;
+        int mat_len = 0;
+        if (op.kind == BK_DENSE) {
+          kind = op.kt == 1 ? RK_DENSE1 : RK_DENSE2;
+          q1 = qpos(op.tmask[0]);
+          q2 = op.kt == 2 ? qpos(op.tmask[1]) : 0;
+          mat_len = (1 << op.kt) * (1 << op.kt);
+        } else if (op.kind == BK_DIAG) {
+          kind = RK_DIAG;
+          dk = static_cast<uint32_t>(op.kt);
+          for (int i = 0; i < op.kt; ++i) dq |= qpos(op.tmask[i]) << (3 * i);
+          mat_len = 1 << op.kt;
+        } else if (op.kt == 1) {
+          if (perm_pool[op.perm_off] == 0) continue;  // identity
+          kind = RK_PERM1;
+          q1 = qpos(op.tmask[0]);
+        } else {
+          kind = RK_PERM2;
+          q1 = qpos(op.tmask[0]);
+          q2 = qpos(op.tmask[1]);
+          for (int i = 0; i < 4; ++i) perm |= static_cast<uint32_t>(perm_pool[op.perm_off + i]) << (2 * i);
+        }
+        ro.w0 = kind | (q1 << 4) | (q2 << 8) | (dk << 12) | (dq << 16);
+        ro.w1 = crm | (ctm << 8) | (perm << 24);
+        ro.w2 = static_cast<uint32_t>(smat);
+        ro.w3 = static_cast<uint32_t>(op.mat_off < 0 ? 0 : op.mat_off);
+        ro.mat_len = mat_len;
+        smat += mat_len;
+        s.rops.push_back(ro);
+      }
+      st.b = static_cast<int32_t>(s.rops.size());
+      s.steps.push_back(st);
+      std::vector<int> left;
+      for (int o : rem)
+        if (std::find(members.begin(), members.end(), o) == members.end()) left.push_back(o);
+      rem.swap(left);
+    }
+    pd.step_end = static_cast<int32_t>(s.steps.size());
+    pd.rop_end = static_cast<int32_t>(s.rops.size());
+    pd.smat_len = smat;
+  }
+}
+
 int default_tile_bits(int nb, int dtype, int maxk, int c_seed, bool adjoint) {
-  int t = (dtype == JQ_C64) ? 14 : 13;
-  if (adjoint) t -= 1;
+  // 64 KB tiles: two CTAs share an SM, so one streams its tile while the
+  // other computes (a 128 KB tile leaves the SM idle during its own copies)
+  // 16 amplitudes per thread, 128 threads per tile: small tiles leave
+  // several CTAs per SM to hide shared-memory and barrier latency
+  int t = 11;
+  if (adjoint) t = 11;
   // keep at least ~256 tiles per state when the state is large enough
   int floor_t = std::max(10, maxk + c_seed);
   if (nb - 8 < t) t = std::max(nb - 8, floor_t);
@@ -527,10 +676,18 @@ int build_plan(const jq_op* ops, int n_ops, const jq_obs* obs, int n_obs, int n_
   plan->fwd = schedule(blocks, plan->blocks, nb, tf, c_seed, no_fuse);
   plan->adj = schedule(blocks, plan->blocks, nb, ta, c_seed, no_fuse);
   plan->bwd = schedule(blocks, plan->blocks, nb, ta, c_seed, true);
+  build_steps(plan->fwd, plan->perm_pool, dtype);
+  build_steps(plan->bwd, plan->perm_pool, dtype);
   plan->threads = (tune && tune->threads > 0) ? tune->threads : 512;
   if (plan->threads % 32 || plan->threads < 64 || plan->threads > 1024)
     return fail("jq_plan_build: threads must be a multiple of 32 in 64..1024");
   plan->ckpt_stride = (tune && tune->ckpt_stride > 0) ? tune->ckpt_stride : 0;
+  {
+    const int mode_jit = tune ? tune->jit : 0;
+    const char* env = std::getenv("JQ_NO_JIT");
+    const bool env_off = env && env[0] && env[0] != '0';
+    plan->jit = !env_off && (mode_jit > 0 || (mode_jit == 0 && nb >= 16));
+  }
 
   // ---- observables -----------------------------------------------------------------
   for (int i = 0; i < n_obs; ++i) {

@@ -355,7 +355,7 @@ def gather_angles(values: list, device: torch.device) -> Optional[torch.Tensor]:
 def gather_mats(values: list, device: torch.device) -> Optional[torch.Tensor]:
     if not values:
         return None
-    parts = [v.to(torch.complex128).reshape(-1).to(device) for v in values]
+    parts = [v.resolve_conj().to(torch.complex128).reshape(-1).to(device) for v in values]
     return torch.cat(parts) if len(parts) > 1 else parts[0]
 
 

@@ -480,3 +480,96 @@ def adam_trajectory(value_and_grad, params: np.ndarray, lr: float, steps: int):
         losses.append(float(loss))
     losses.append(float(value_and_grad(p)[0]))
     return np.array(losses), p
+
+
+# ---------------------------------------------------------------------------
+# the reference's executable plan with matrices (simulation.py:214-335), for
+# the timed CPU baseline (oracle/jqoracle.c executes it)
+# ---------------------------------------------------------------------------
+def _structure(name: str, k: int):
+    if name in STRUCT_PERM:
+        return ("perm", STRUCT_PERM[name])
+    if name in STRUCT_DIAG:
+        return ("diag", None)
+    return (None, None)
+
+
+def _fused_kind(a, b):
+    if a[0] == "perm" and b[0] == "perm":
+        return ("perm", tuple(a[1][i] for i in b[1]))
+    if a[0] == "diag" and b[0] == "diag":
+        return ("diag", None)
+    return (None, None)
+
+
+def compose_permutation(blocks, n: int) -> np.ndarray:
+    """2^n int32 gather map of a run of permutation blocks (:243-267):
+    out[o] = in[index[o]]."""
+    o = np.arange(2**n, dtype=np.int64)
+    index = o.copy()
+    for _, wires, (_, perm) in blocks:
+        k = len(wires)
+        bits = [n - 1 - w for w in wires]
+        col = np.zeros_like(o)
+        mask = 0
+        for i, b in enumerate(bits):
+            col |= ((o >> b) & 1) << (k - 1 - i)
+            mask |= 1 << b
+        src_col = np.asarray(perm, dtype=np.int64)[col]
+        src = o & ~mask
+        for i, b in enumerate(bits):
+            src |= ((src_col >> (k - 1 - i)) & 1) << b
+        index = index[src]
+    return index.astype(np.int32)
+
+
+def jaqsi_plan(records, n: int):
+    """Entries ('dense', wires, U) | ('gather', index) | ('diag', wires, d) of
+    jaqsi's statevector plan: _fuse then _fuse_runs."""
+    blocks: List[list] = []
+    last: Dict[int, int] = {}
+    for name, wires, params in records:
+        if name == "Barrier":
+            continue
+        wires = tuple(wires)
+        U = gate_matrix(name, params, len(wires))
+        st = _structure(name, len(wires))
+        i = last.get(wires[0])
+        if i is not None and blocks[i][1] == wires and all(last[w] == i for w in wires):
+            blocks[i][0] = U @ blocks[i][0]
+            blocks[i][2] = _fused_kind(blocks[i][2], st)
+            continue
+        blocks.append([U, wires, st])
+        for w in wires:
+            last[w] = len(blocks) - 1
+    plan = []
+    run: List[list] = []
+    kind = None
+
+    def flush():
+        if len(run) > 1 and kind == "perm":
+            plan.append(("gather", compose_permutation(run, n)))
+        elif len(run) > 1:
+            ws = tuple(sorted({w for b in run for w in b[1]}))
+            d = np.ones((2,) * len(ws), dtype=np.complex128)
+            ax = {w: i for i, w in enumerate(ws)}
+            for U, bw, _ in run:
+                f = np.diag(U).reshape((2,) * len(bw) + (1,) * (len(ws) - len(bw)))
+                d = d * np.moveaxis(f, tuple(range(len(bw))), tuple(ax[w] for w in bw))
+            plan.append(("diag", ws, d.reshape(-1)))
+        else:
+            for U, bw, _ in run:
+                plan.append(("dense", bw, U))
+        run.clear()
+
+    for b in blocks:
+        k = b[2][0]
+        if k != kind:
+            flush()
+            kind = k
+        if k is None:
+            plan.append(("dense", b[1], b[0]))
+        else:
+            run.append(b)
+    flush()
+    return plan
