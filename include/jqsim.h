@@ -210,6 +210,28 @@ JQ_API int jq_sweep(const jq_plan* plan, int batch, const double* angles,
                     const void* mats, void* state, void* workspace,
                     size_t workspace_bytes, void* stream);
 
+/* jq_forward without any device allocation, for callers that cannot
+ * allocate device memory: hosts that bind this C ABI holding only raw device
+ * pointers and no allocator (an FFI host whose memory belongs to another
+ * runtime), and services running under a fixed device-memory budget that must
+ * not grow at run time.  No counterpart in the reference (jaqsi allocates
+ * through XLA).
+ *
+ * The workspace is a file-scope static device array of JQ_STATIC_WS_BYTES
+ * (4 MiB) that every GPU loading the library holds until exit; plans whose
+ * forward workspace for `batch` instances exceeds it are rejected with
+ * JQ_ENOMEM.  The plan's tables must already be resident on the current device
+ * (one prior jq_forward / jq_adjoint / jq_backward / jq_sweep on that device),
+ * otherwise JQ_EINVAL.  The first call on a device resolves the array's
+ * address (cudaGetSymbolAddress); make that first call before any stream
+ * capture.  All calls share the array and it keeps the last call's contents,
+ * so calls that overlap on the GPU (other streams, other threads) race:
+ * serialise them.  Arguments and results are those of jq_forward. */
+#define JQ_STATIC_WS_BYTES (4u << 20)
+JQ_API int jq_forward_noalloc(const jq_plan* plan, int batch, const double* angles,
+                              const void* mats, const void* init, int init_batched,
+                              int out_type, void* state, void* out, void* stream);
+
 /* Adjoint-method gradient of the expectation values of a unitary pure-state
  * plan, O(1) extra statevectors.  Replaces jaqsi/simulation.py:546-655
  * (_adjoint_expval).  `state` holds the forward result (it is left intact).

@@ -20,6 +20,7 @@ JQ_EUNSUPPORTED = -6
 
 JQ_MAX_OP_WIRES = 6
 JQ_MAX_QUBITS = 30
+JQ_STATIC_WS_BYTES = 4 << 20
 
 JQ_C64, JQ_C128 = 0, 1
 JQ_STATEVECTOR, JQ_DENSITY = 0, 1
@@ -46,6 +47,7 @@ EXPORTED = (
     "jq_plan_jit_source",
     "jq_workspace_bytes",
     "jq_forward",
+    "jq_forward_noalloc",
     "jq_sweep",
     "jq_adjoint",
     "jq_backward",
@@ -150,6 +152,8 @@ def _declare(lib: ctypes.CDLL) -> None:
     lib.jq_workspace_bytes.restype = ctypes.c_size_t
     lib.jq_forward.argtypes = [vp, i32, vp, vp, vp, i32, i32, vp, vp, vp, ctypes.c_size_t, vp]
     lib.jq_forward.restype = i32
+    lib.jq_forward_noalloc.argtypes = [vp, i32, vp, vp, vp, i32, i32, vp, vp, vp]
+    lib.jq_forward_noalloc.restype = i32
     lib.jq_sweep.argtypes = [vp, i32, vp, vp, vp, vp, ctypes.c_size_t, vp]
     lib.jq_sweep.restype = i32
     lib.jq_adjoint.argtypes = [vp, i32, vp, vp, vp, i32, vp, vp, vp, vp, vp, vp, ctypes.c_size_t, vp]

@@ -2332,6 +2332,61 @@ int jq_backward(const jq_plan* plan, int batch, const double* angles, const void
                                grad_mats, grad_init, workspace, workspace_bytes, st);
 }
 
+}  // extern "C"
+
+// Workspace of jq_forward_noalloc: a file-scope device array, so that entry
+// point performs no allocation.  Host code cannot use the symbol as a device
+// address; its address is resolved per device with cudaGetSymbolAddress.
+static __device__ __align__(256) unsigned char g_noalloc_ws[JQ_STATIC_WS_BYTES];
+
+namespace {
+std::mutex g_noalloc_mu;
+std::vector<std::pair<int, void*>> g_noalloc_ptr;  // (device, address of g_noalloc_ws)
+}  // namespace
+
+extern "C" {
+
+int jq_forward_noalloc(const jq_plan* plan, int batch, const double* angles, const void* mats, const void* init,
+                       int init_batched, int out_type, void* state, void* out, void* stream) {
+  int rc = check_common(plan, batch, angles, mats);
+  if (rc) return rc;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    set_error("jq_forward_noalloc: no current CUDA device");
+    return JQ_ECUDA;
+  }
+  bool resident = false;
+  for (const DeviceTables& t : plan->dev) resident = resident || t.device == dev;
+  if (!resident) {
+    set_error("jq_forward_noalloc: the plan is not resident on this device; run jq_forward (or another "
+              "execution entry point) with it once on this device first");
+    return JQ_EINVAL;
+  }
+  const size_t need = layout(plan, batch, 0).total;
+  if (need > JQ_STATIC_WS_BYTES) {
+    set_error("jq_forward_noalloc: the plan needs " + std::to_string(need) + " workspace bytes for batch " +
+              std::to_string(batch) + ", above the static limit of " + std::to_string(JQ_STATIC_WS_BYTES) +
+              " bytes; use jq_forward with a caller-provided workspace");
+    return JQ_ENOMEM;
+  }
+  void* ws = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    for (const auto& e : g_noalloc_ptr)
+      if (e.first == dev) ws = e.second;
+    if (!ws) {
+      const cudaError_t e = cudaGetSymbolAddress(&ws, g_noalloc_ws);
+      if (e != cudaSuccess || !ws) {
+        set_error(std::string("jq_forward_noalloc: cudaGetSymbolAddress failed: ") + cudaGetErrorString(e));
+        return JQ_ECUDA;
+      }
+      g_noalloc_ptr.emplace_back(dev, ws);
+    }
+  }
+  return jq_forward(plan, batch, angles, mats, init, init_batched, out_type, state, out, ws, JQ_STATIC_WS_BYTES,
+                    stream);
+}
+
 const char* jq_last_error(void) { return g_last_error.c_str(); }
 
 const char* jq_version(void) { return "jqsim 0.1.0 (sm_100a)"; }
