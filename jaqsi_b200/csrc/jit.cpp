@@ -152,6 +152,42 @@ __device__ __forceinline__ void store16(const double2* s, double2* g, const u32*
     for (int u = 0; u < B; ++u) { const int v = v0 + u * blockDim.x; if (v < nv) __stcs(g + (tbl[v >> c] | (v & cm)), r[u]); }
   }
 }
+// Warp reduce-scatter of N (power of two, <= 32) per-lane partial sums by
+// recursive halving: at the step exchanging with lane ^ o the lanes with bit o
+// set keep the upper half of the remaining values.  N - 1 shuffles for the
+// halving steps plus one per remaining lane bit; afterwards the top log2(N)
+// lane bits index the value a lane holds and the lanes whose low bits are zero
+// add it into dst[index] (float64 shared accumulators).
+template <int O, int N, typename F> struct WarpRS {
+  static __device__ __forceinline__ void run(F* v, unsigned lane) {
+    if constexpr (N > 1) {
+      constexpr int h = N / 2;
+      const bool up = (lane & O) != 0;
+#pragma unroll
+      for (int i = 0; i < h; ++i) {
+        const F send = up ? v[i] : v[i + h];
+        const F keep = up ? v[i + h] : v[i];
+        v[i] = keep + __shfl_xor_sync(0xffffffffu, send, O);
+      }
+      if constexpr (O > 1) WarpRS<O / 2, h, F>::run(v, lane);
+    } else {
+      v[0] += __shfl_xor_sync(0xffffffffu, v[0], O);
+      if constexpr (O > 1) WarpRS<O / 2, 1, F>::run(v, lane);
+    }
+  }
+};
+template <int N, typename F> __device__ __forceinline__ void warp_rs_add(F (&v)[N], double* dst) {
+  const unsigned lane = threadIdx.x & 31u;
+  WarpRS<16, N, F>::run(v, lane);
+  constexpr int lg = (N >= 32) ? 5 : (N >= 16) ? 4 : (N >= 8) ? 3 : (N >= 4) ? 2 : (N >= 2) ? 1 : 0;
+  if ((lane & ((32u >> lg) - 1u)) == 0) atomicAdd(dst + (lane >> (5 - lg)), (double)v[0]);
+}
+template <typename C> __device__ __forceinline__ C cconj(C a) { a.y = -a.y; return a; }
+// a * conj(b)
+template <typename C> __device__ __forceinline__ C cmulc(C a, C b) {
+  C r; r.x = a.x * b.x + a.y * b.y; r.y = a.y * b.x - a.x * b.y; return r;
+}
+template <typename C> __device__ __forceinline__ C cadd(C a, C b) { a.x += b.x; a.y += b.y; return a; }
 )JQ";
 
 std::string hex(uint64_t v) {
@@ -167,7 +203,9 @@ void emit_pass(std::ostringstream& o, const jq_plan* plan, const Schedule& s, in
   const int t = pd.t, c = pd.c, nb = plan->n_bits;
   const int nthr = 1 << (t - rb);
   const int nr = 1 << rb;
-  const int minb = std::max(1, std::min(8, 65536 / (nthr * 128)));
+  // register budget: 16 complex64 amplitudes + a 4x4 matrix fit 128 registers;
+  // complex128 needs about 168
+  const int minb = std::max(1, std::min(8, 65536 / (nthr * (c64 ? 128 : 168))));
   const uint64_t full = (nb >= 64) ? ~0ULL : ((1ULL << nb) - 1);
   const uint64_t outer = full & ~pd.tile_mask;
   const int smat_pad = (pd.smat_len + 1) & ~1;
@@ -308,6 +346,231 @@ void emit_pass(std::ostringstream& o, const jq_plan* plan, const Schedule& s, in
   o << "  }\n}\n";
 }
 
+// Emit the adjoint kernel of pass p: the pass's register stages in reverse,
+// psi <- G^dagger psi, block cotangent += lam psi^dagger (float64 shared
+// accumulators, flushed to the global accumulator per instance), lam <- G^dagger lam.
+void emit_adj_pass(std::ostringstream& o, const jq_plan* plan, const Schedule& s, int p, bool c64, int rb) {
+  const PassDesc& pd = s.passes[p];
+  const char* T = c64 ? "float2" : "double2";
+  const int t = pd.t, c = pd.c, nb = plan->n_bits;
+  const int nthr = 1 << (t - rb);
+  const int nr = 1 << rb;
+  // both tiles' register blocks are live: allow up to 255 registers a thread
+  const int minb = std::max(1, std::min(8, 65536 / (nthr * 256)));
+  const uint64_t full = (nb >= 64) ? ~0ULL : ((1ULL << nb) - 1);
+  const uint64_t outer = full & ~pd.tile_mask;
+  const int smat_pad = (pd.smat_len + 1) & ~1;
+  const char* F = c64 ? "float" : "double";
+  int nmc = 0, ngt = 0, nacc = 0;
+  std::vector<int> acc_off(pd.rop_end - pd.rop_begin, -1);
+  for (int ri = pd.rop_begin; ri < pd.rop_end; ++ri) {
+    const RegOp& ro = s.rops[ri];
+    nmc += ro.mat_len > 0;
+    if (ro.grad_off >= 0) {
+      acc_off[ri - pd.rop_begin] = nacc;
+      nacc += 2 * ro.mat_len;  // re/im of each entry of the inner matrix / diagonal
+      ++ngt;
+    }
+  }
+  const int nacc_pad = (nacc + 1) & ~1;
+  o << "extern \"C\" __global__ void __launch_bounds__(" << nthr << ", " << minb << ") @KERNEL@(" << T
+    << "* __restrict__ psi, " << T << "* __restrict__ lam, int batch, const " << T
+    << "* __restrict__ bmat, long long bstride, const int* __restrict__ mc, double* __restrict__ gacc, "
+    << "long long gstride, const int* __restrict__ gt) {\n";
+  o << "  extern __shared__ __align__(16) unsigned char smem[];\n";
+  o << "  " << T << "* sp = (" << T << "*)smem;\n";
+  o << "  " << T << "* sl = sp + " << (1 << t) << ";\n";
+  o << "  " << T << "* smat = sl + " << (1 << t) << ";\n";
+  o << "  double* sacc = (double*)(smat + " << smat_pad << ");\n";
+  o << "  u32* tbl = (u32*)(sacc + " << nacc_pad << ");\n";
+  o << "  const u32 tid = threadIdx.x;\n";
+  o << "  { const u32 hb[] = {";
+  for (int i = c; i < t; ++i) o << (i > c ? ", " : "") << (1u << pd.bits[i]);
+  if (t == c) o << "0u";
+  o << "};\n    for (int h = tid; h < " << (1 << (t - c)) << "; h += blockDim.x) { u32 v = 0;";
+  o << " for (int i = 0; i < " << (t - c) << "; ++i) if ((h >> i) & 1) v |= hb[i]; tbl[h] = v; } }\n";
+  o << "  for (int e = tid; e < " << nacc_pad << "; e += blockDim.x) sacc[e] = 0.0;\n";
+  int nstage = 0;
+  for (int si = pd.step_begin; si < pd.step_end; ++si) {
+    const Step& st = s.steps[si];
+    o << "  u32 tb" << nstage << " = 0;";
+    for (int i = 0; i < t - rb; ++i) o << " if (tid & " << (1u << i) << "u) tb" << nstage << " ^= " << st.tbits[i] << "u;";
+    o << "\n";
+    ++nstage;
+  }
+  // flush of the shared accumulators into the instance's global accumulator
+  // (skipped when the caller wants no parameter gradient: gacc is NULL)
+  auto flush_for = [&](const std::string& inst) {
+    return "      if (gacc) for (int i = 0; i < " + std::to_string(ngt) +
+           "; ++i) { const int so = gt[3 * i], go = gt[3 * i + 1], n = gt[3 * i + 2];\n"
+           "        for (int e = tid; e < n; e += blockDim.x) atomicAdd(&gacc[" + inst +
+           " * gstride * 2 + 2 * go + e], sacc[so + e]); }\n";
+  };
+  o << "  const long long tiles_per = 1ll << " << (nb - t) << ";\n";
+  o << "  const long long ntiles = tiles_per * batch;\n";
+  o << "  long long last_inst = -1;\n";
+  o << "  for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {\n";
+  o << "    const long long inst = tile >> " << (nb - t) << ";\n";
+  o << "    const u64 ti = (u64)tile & (u64)(tiles_per - 1);\n";
+  o << "    const long long goff = (inst << " << nb << ") + (long long)pdep64(ti, " << hex(outer) << ");\n";
+  o << "    __syncthreads();\n";
+  o << "    if (inst != last_inst) {\n";
+  o << "      if (last_inst >= 0) {\n" << flush_for("last_inst") << "        __syncthreads();\n";
+  o << "        for (int e = tid; e < " << nacc_pad << "; e += blockDim.x) sacc[e] = 0.0;\n      }\n";
+  o << "      const " << T << "* bm = bmat + inst * bstride;\n";
+  o << "      for (int i = 0; i < " << nmc << "; ++i) { const int d = mc[3 * i], a = mc[3 * i + 1], n = mc[3 * i + 2];\n";
+  o << "        for (int e = tid; e < n; e += blockDim.x) smat[d + e] = bm[a + e]; }\n";
+  o << "      (void)bm; last_inst = inst;\n      __syncthreads();\n    }\n";
+  o << "    " << (c64 ? "load8<4>" : "load16<2>") << "(sp, psi + goff, tbl, " << t << ", " << c << ");\n";
+  o << "    " << (c64 ? "load8<4>" : "load16<2>") << "(sl, lam + goff, tbl, " << t << ", " << c << ");\n";
+  o << "    __syncthreads();\n";
+  for (int si = pd.step_end - 1; si >= pd.step_begin; --si) {
+    const int k = si - pd.step_begin;
+    const Step& st = s.steps[si];
+    std::vector<uint32_t> off(nr);
+    for (int j = 0; j < nr; ++j) {
+      uint32_t a = 0;
+      for (int q = 0; q < rb; ++q)
+        if ((j >> q) & 1) a ^= st.ebits[q];
+      off[j] = a;
+    }
+    std::vector<int> var(nr);
+    for (int j = 0; j < nr; ++j) var[j] = j;
+    o << "    {\n";
+    for (int j = 0; j < nr; ++j) {
+      o << "      " << T << " p" << j << " = sp[tb" << k << " ^ " << off[j] << "u];";
+      o << " " << T << " l" << j << " = sl[tb" << k << " ^ " << off[j] << "u];\n";
+    }
+    for (int ri = st.b - 1; ri >= st.a; --ri) {
+      const RegOp& ro = s.rops[ri];
+      const uint32_t kind = ro.w0 & 15u, q1 = (ro.w0 >> 4) & 15u, q2 = (ro.w0 >> 8) & 15u;
+      const uint32_t dk = (ro.w0 >> 12) & 15u, dq = ro.w0 >> 16;
+      const uint32_t crm = ro.w1 & 0xFFu, ctm = (ro.w1 >> 8) & 0xFFFFu, perm = ro.w1 >> 24;
+      const uint32_t M = ro.w2;
+      const bool guard = ctm != 0;
+      const bool grad = ro.grad_off >= 0;
+      const int ao = acc_off[ri - pd.rop_begin];
+      auto P = [&](int j) { return std::string("p") + std::to_string(var[j]); };
+      auto Lm = [&](int j) { return std::string("l") + std::to_string(var[j]); };
+      o << "      {\n";
+      int ng = 0;
+      if (grad) {
+        ng = (kind == RK_DIAG) ? (1 << dk) : (kind == RK_DENSE1 ? 4 : 16);
+        o << "        " << T << " g[" << ng << "];\n        for (int e = 0; e < " << ng
+          << "; ++e) { g[e].x = 0; g[e].y = 0; }\n";
+      }
+      if (guard) o << "        if ((tid & " << ctm << "u) == " << ctm << "u) {\n";
+      else o << "        {\n";
+      if (kind == RK_DENSE1) {
+        // G^dagger = [[conj m00, conj m10], [conj m01, conj m11]]
+        o << "          const " << T << " h00 = cconj(smat[" << M << "]), h01 = cconj(smat[" << M + 2
+          << "]), h10 = cconj(smat[" << M + 1 << "]), h11 = cconj(smat[" << M + 3 << "]);\n";
+        for (int j = 0; j < nr; ++j) {
+          if ((j >> q1) & 1) continue;
+          if ((static_cast<uint32_t>(j) & crm) != crm) continue;
+          const int kk = j | (1 << q1);
+          o << "          { const " << T << " x = " << P(j) << ", y = " << P(kk) << "; " << P(j)
+            << " = cfma(h01, y, cmul(h00, x)); " << P(kk) << " = cfma(h11, y, cmul(h10, x));\n";
+          if (grad)
+            o << "            g[0] = cadd(g[0], cmulc(" << Lm(j) << ", " << P(j) << ")); g[1] = cadd(g[1], cmulc(" << Lm(j)
+              << ", " << P(kk) << ")); g[2] = cadd(g[2], cmulc(" << Lm(kk) << ", " << P(j)
+              << ")); g[3] = cadd(g[3], cmulc(" << Lm(kk) << ", " << P(kk) << "));\n";
+          o << "            const " << T << " u = " << Lm(j) << ", w = " << Lm(kk) << "; " << Lm(j)
+            << " = cfma(h01, w, cmul(h00, u)); " << Lm(kk) << " = cfma(h11, w, cmul(h10, u)); }\n";
+        }
+      } else if (kind == RK_PERM1) {
+        for (int j = 0; j < nr; ++j) {
+          if ((j >> q1) & 1) continue;
+          if ((static_cast<uint32_t>(j) & crm) != crm) continue;
+          const int kk = j | (1 << q1);
+          if (!guard) {
+            std::swap(var[j], var[kk]);
+          } else {
+            o << "          { " << T << " x = " << P(j) << "; " << P(j) << " = " << P(kk) << "; " << P(kk)
+              << " = x; x = " << Lm(j) << "; " << Lm(j) << " = " << Lm(kk) << "; " << Lm(kk) << " = x; }\n";
+          }
+        }
+      } else if (kind == RK_DIAG) {
+        for (int j = 0; j < nr; ++j) {
+          if ((static_cast<uint32_t>(j) & crm) != crm) continue;
+          int idx = 0;
+          for (uint32_t i = 0; i < dk; ++i) idx = (idx << 1) | ((j >> ((dq >> (3 * i)) & 7u)) & 1);
+          o << "          { const " << T << " d = cconj(smat[" << M + idx << "]); " << P(j) << " = cmul(d, " << P(j)
+            << ");";
+          if (grad) o << " g[" << idx << "] = cadd(g[" << idx << "], cmulc(" << Lm(j) << ", " << P(j) << "));";
+          o << " " << Lm(j) << " = cmul(d, " << Lm(j) << "); }\n";
+        }
+      } else if (kind == RK_DENSE2) {
+        for (int j = 0; j < nr; ++j) {
+          if (((j >> q1) & 1) || ((j >> q2) & 1)) continue;
+          if ((static_cast<uint32_t>(j) & crm) != crm) continue;
+          const int id[4] = {j, j | (1 << q2), j | (1 << q1), j | (1 << q1) | (1 << q2)};
+          o << "          { const " << T << " a0 = " << P(id[0]) << ", a1 = " << P(id[1]) << ", a2 = " << P(id[2])
+            << ", a3 = " << P(id[3]) << ";\n";
+          // (G^dagger)[r][q] = conj(G[q][r]), read from shared memory each time
+          auto H = [&](int r, int q) { return "cconj(smat[" + std::to_string(M + 4 * q + r) + "])"; };
+          for (int r = 0; r < 4; ++r)
+            o << "            " << P(id[r]) << " = cfma(" << H(r, 3) << ", a3, cfma(" << H(r, 2) << ", a2, cfma("
+              << H(r, 1) << ", a1, cmul(" << H(r, 0) << ", a0))));\n";
+          if (grad)
+            for (int r = 0; r < 4; ++r)
+              for (int q = 0; q < 4; ++q)
+                o << "            g[" << 4 * r + q << "] = cadd(g[" << 4 * r + q << "], cmulc(" << Lm(id[r]) << ", "
+                  << P(id[q]) << "));\n";
+          o << "            const " << T << " b0 = " << Lm(id[0]) << ", b1 = " << Lm(id[1]) << ", b2 = " << Lm(id[2])
+            << ", b3 = " << Lm(id[3]) << ";\n";
+          for (int r = 0; r < 4; ++r)
+            o << "            " << Lm(id[r]) << " = cfma(" << H(r, 3) << ", b3, cfma(" << H(r, 2) << ", b2, cfma("
+              << H(r, 1) << ", b1, cmul(" << H(r, 0) << ", b0))));\n";
+          o << "          }\n";
+        }
+      } else {  // RK_PERM2, inverse: new[p[r]] = old[r]
+        for (int j = 0; j < nr; ++j) {
+          if (((j >> q1) & 1) || ((j >> q2) & 1)) continue;
+          if ((static_cast<uint32_t>(j) & crm) != crm) continue;
+          const int id[4] = {j, j | (1 << q2), j | (1 << q1), j | (1 << q1) | (1 << q2)};
+          int pv[4];
+          for (int r = 0; r < 4; ++r) pv[r] = (perm >> (2 * r)) & 3u;
+          if (!guard) {
+            int nv[4];
+            for (int r = 0; r < 4; ++r) nv[pv[r]] = var[id[r]];
+            for (int r = 0; r < 4; ++r) var[id[r]] = nv[r];
+          } else {
+            o << "          { const " << T << " a0 = " << P(id[0]) << ", a1 = " << P(id[1]) << ", a2 = " << P(id[2])
+              << ", a3 = " << P(id[3]) << ";";
+            for (int r = 0; r < 4; ++r) o << " " << P(id[pv[r]]) << " = a" << r << ";";
+            o << " }\n";
+            o << "          { const " << T << " a0 = " << Lm(id[0]) << ", a1 = " << Lm(id[1]) << ", a2 = " << Lm(id[2])
+              << ", a3 = " << Lm(id[3]) << ";";
+            for (int r = 0; r < 4; ++r) o << " " << Lm(id[pv[r]]) << " = a" << r << ";";
+            o << " }\n";
+          }
+        }
+      }
+      o << "        }\n";
+      if (grad) {
+        // reduce the warp's partial cotangent, 32 values at a time
+        const int nv = 2 * ng;
+        for (int c0 = 0; c0 < nv; c0 += 32) {
+          const int cn = std::min(32, nv - c0);
+          o << "        { " << F << " vv[" << cn << "] = {";
+          for (int e = 0; e < cn; ++e)
+            o << (e ? ", " : "") << "g[" << (c0 + e) / 2 << "]." << (((c0 + e) & 1) ? "y" : "x");
+          o << "}; warp_rs_add<" << cn << ">(vv, &sacc[" << ao + c0 << "]); }\n";
+        }
+      }
+      o << "      }\n";
+    }
+    for (int j = 0; j < nr; ++j)
+      o << "      sp[tb" << k << " ^ " << off[j] << "u] = p" << var[j] << "; sl[tb" << k << " ^ " << off[j]
+        << "u] = l" << var[j] << ";\n";
+    o << "    }\n    __syncthreads();\n";
+  }
+  o << "    " << (c64 ? "store8<4>" : "store16<2>") << "(sp, psi + goff, tbl, " << t << ", " << c << ");\n";
+  o << "    " << (c64 ? "store8<4>" : "store16<2>") << "(sl, lam + goff, tbl, " << t << ", " << c << ");\n";
+  o << "  }\n  __syncthreads();\n  if (last_inst >= 0) {\n" << flush_for("last_inst") << "  }\n}\n";
+}
+
 }  // namespace
 
 bool jit_available() {
@@ -323,17 +586,17 @@ bool jit_pass_eligible(const Schedule& s, int p) {
   return true;
 }
 
-// Kernel text of every eligible pass; identical texts share one kernel.
-void emit_all(const jq_plan* plan, const Schedule& s, std::string* src, std::vector<int>* kernel_of,
-              std::vector<std::string>* names) {
-  std::ostringstream all;
-  all << kPrelude;
+// Kernel text of every eligible pass (forward, or adjoint when `adjoint`);
+// identical texts share one kernel.  Appends to `all`, names kernels prefix + k.
+void emit_kernels(const jq_plan* plan, const Schedule& s, bool adjoint, const char* prefix, std::ostringstream& all,
+                  std::vector<int>* kernel_of, std::vector<std::string>* names) {
   kernel_of->assign(s.passes.size(), -1);
   std::vector<std::string> texts;
   for (int p = 0; p < static_cast<int>(s.passes.size()); ++p) {
     if (!jit_pass_eligible(s, p)) continue;
     std::ostringstream o;
-    emit_pass(o, plan, s, p, plan->dtype == JQ_C64, s.reg_bits);
+    if (adjoint) emit_adj_pass(o, plan, s, p, plan->dtype == JQ_C64, s.reg_bits);
+    else emit_pass(o, plan, s, p, plan->dtype == JQ_C64, s.reg_bits);
     const std::string text = o.str();
     int k = -1;
     for (size_t i = 0; i < texts.size(); ++i)
@@ -341,7 +604,7 @@ void emit_all(const jq_plan* plan, const Schedule& s, std::string* src, std::vec
     if (k < 0) {
       k = static_cast<int>(texts.size());
       texts.push_back(text);
-      const std::string name = "jqk" + std::to_string(k);
+      const std::string name = prefix + std::to_string(k);
       names->push_back(name);
       std::string body = text;
       body.replace(body.find("@KERNEL@"), 8, name);
@@ -349,15 +612,20 @@ void emit_all(const jq_plan* plan, const Schedule& s, std::string* src, std::vec
     }
     (*kernel_of)[p] = k;
   }
-  *src = all.str();
 }
 
+// The adjoint kernels are specialised too when the plan can run jq_adjoint
+// (a unitary statevector plan).
+bool plan_wants_adjoint(const jq_plan* plan) { return plan->mode == JQ_STATEVECTOR && plan->unitary; }
+
 std::string jit_source(const jq_plan* plan, const Schedule& s) {
-  std::string src;
+  std::ostringstream all;
+  all << kPrelude;
   std::vector<int> kernel_of;
   std::vector<std::string> names;
-  emit_all(plan, s, &src, &kernel_of, &names);
-  return src;
+  emit_kernels(plan, s, false, "jqk", all, &kernel_of, &names);
+  if (plan_wants_adjoint(plan)) emit_kernels(plan, s, true, "jqa", all, &kernel_of, &names);
+  return all.str();
 }
 
 int jit_build(const jq_plan* plan, const Schedule& s, JitModule* out) {
@@ -365,14 +633,21 @@ int jit_build(const jq_plan* plan, const Schedule& s, JitModule* out) {
     set_error("NVRTC or the CUDA driver entry points are not available");
     return JQ_EUNSUPPORTED;
   }
-  std::string src;
-  std::vector<int> kernel_of;
-  std::vector<std::string> names;
-  emit_all(plan, s, &src, &kernel_of, &names);
+  std::ostringstream all;
+  all << kPrelude;
+  std::vector<int> kernel_of, akernel_of;
+  std::vector<std::string> names, anames;
+  emit_kernels(plan, s, false, "jqk", all, &kernel_of, &names);
+  const bool adj = plan_wants_adjoint(plan);
+  if (adj) emit_kernels(plan, s, true, "jqa", all, &akernel_of, &anames);
+  const std::string src = all.str();
   out->fn.assign(s.passes.size(), nullptr);
+  out->afn.assign(s.passes.size(), nullptr);
   out->module = nullptr;
   out->mc = nullptr;
+  out->gt = nullptr;
   out->mc_off.assign(s.passes.size(), 0);
+  out->gt_off.assign(s.passes.size(), 0);
   if (names.empty()) return JQ_OK;
   nvrtcProgram prog;
   if (g_nvrtc.create(&prog, src.c_str(), "jq_plan.cu", 0, nullptr, nullptr) != NVRTC_SUCCESS) {
@@ -401,25 +676,42 @@ int jit_build(const jq_plan* plan, const Schedule& s, JitModule* out) {
     return JQ_ECUDA;
   }
   out->module = mod;
-  std::vector<void*> fk(names.size(), nullptr);
-  for (size_t k = 0; k < names.size(); ++k) {
-    CUfunction f;
-    if (g_drv.get_function(&f, mod, names[k].c_str()) != CUDA_SUCCESS) {
-      set_error("cuModuleGetFunction failed for " + names[k]);
-      return JQ_ECUDA;
+  auto lookup = [&](const std::vector<std::string>& nm, std::vector<void*>* fk) -> int {
+    fk->assign(nm.size(), nullptr);
+    for (size_t k = 0; k < nm.size(); ++k) {
+      CUfunction f;
+      if (g_drv.get_function(&f, mod, nm[k].c_str()) != CUDA_SUCCESS) {
+        set_error("cuModuleGetFunction failed for " + nm[k]);
+        return JQ_ECUDA;
+      }
+      g_drv.set_attr(f, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, 227 * 1024);
+      (*fk)[k] = f;
     }
-    g_drv.set_attr(f, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, 227 * 1024);
-    fk[k] = f;
-  }
+    return JQ_OK;
+  };
+  std::vector<void*> fk, ak;
+  if (lookup(names, &fk) || lookup(anames, &ak)) return JQ_ECUDA;
   // per-pass matrix staging tables
   std::vector<int32_t> mc;
+  // per-pass gradient flush tables: (shared accumulator offset, block
+  // cotangent offset in complex128 units, number of doubles)
+  std::vector<int32_t> gt;
   for (int p = 0; p < static_cast<int>(s.passes.size()); ++p) {
     if (kernel_of[p] < 0) continue;
     out->fn[p] = fk[kernel_of[p]];
+    if (adj && akernel_of[p] >= 0) out->afn[p] = ak[akernel_of[p]];
     out->mc_off[p] = static_cast<int64_t>(mc.size());
+    out->gt_off[p] = static_cast<int64_t>(gt.size());
     const PassDesc& pd = s.passes[p];
+    int acc = 0;
     for (int ri = pd.rop_begin; ri < pd.rop_end; ++ri) {
       const RegOp& ro = s.rops[ri];
+      if (ro.grad_off >= 0) {
+        gt.push_back(acc);
+        gt.push_back(ro.grad_off);
+        gt.push_back(2 * ro.mat_len);
+        acc += 2 * ro.mat_len;
+      }
       if (ro.mat_len <= 0) continue;
       mc.push_back(static_cast<int32_t>(ro.w2));
       mc.push_back(static_cast<int32_t>(ro.w3));
@@ -427,11 +719,15 @@ int jit_build(const jq_plan* plan, const Schedule& s, JitModule* out) {
     }
   }
   if (mc.empty()) mc.push_back(0);
+  if (gt.empty()) gt.push_back(0);
   if (cudaMalloc(&out->mc, mc.size() * sizeof(int32_t)) != cudaSuccess ||
-      cudaMemcpy(out->mc, mc.data(), mc.size() * sizeof(int32_t), cudaMemcpyHostToDevice) != cudaSuccess) {
+      cudaMemcpy(out->mc, mc.data(), mc.size() * sizeof(int32_t), cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMalloc(&out->gt, gt.size() * sizeof(int32_t)) != cudaSuccess ||
+      cudaMemcpy(out->gt, gt.data(), gt.size() * sizeof(int32_t), cudaMemcpyHostToDevice) != cudaSuccess) {
     set_error("upload of the matrix staging tables failed");
     return JQ_ECUDA;
   }
+  out->has_adjoint = adj && !anames.empty();
   out->n_kernels = static_cast<int>(names.size());
   return JQ_OK;
 }
@@ -439,8 +735,11 @@ int jit_build(const jq_plan* plan, const Schedule& s, JitModule* out) {
 void jit_free(JitModule* m) {
   if (m && m->module && g_drv.ok) g_drv.module_unload(static_cast<CUmodule>(m->module));
   if (m && m->mc) cudaFree(m->mc);
+  if (m && m->gt) cudaFree(m->gt);
   if (m) {
     m->mc = nullptr;
+    m->gt = nullptr;
+    m->afn.clear();
     m->module = nullptr;
     m->fn.clear();
   }
@@ -470,6 +769,44 @@ int jit_launch(const JitModule& m, const Schedule& s, int p, int n_bits, int sm_
   if (g_drv.launch(f, grid, 1, 1, threads, 1, 1, static_cast<unsigned>(smem), reinterpret_cast<CUstream>(st), args,
                    nullptr) != CUDA_SUCCESS) {
     set_error("cuLaunchKernel failed for a specialised pass");
+    return JQ_ECUDA;
+  }
+  return JQ_OK;
+}
+
+}  // namespace jq
+
+namespace jq {
+
+size_t jit_adj_smem(const Schedule& s, int p, int elem) {
+  const PassDesc& pd = s.passes[p];
+  int nacc = 0;
+  for (int ri = pd.rop_begin; ri < pd.rop_end; ++ri)
+    if (s.rops[ri].grad_off >= 0) nacc += 2 * s.rops[ri].mat_len;
+  return 2 * (static_cast<size_t>(1) << pd.t) * elem + static_cast<size_t>((pd.smat_len + 1) & ~1) * elem +
+         static_cast<size_t>((nacc + 1) & ~1) * 8 + (static_cast<size_t>(1) << (pd.t - pd.c)) * 4;
+}
+
+int jit_launch_adj(const JitModule& m, const Schedule& s, int p, int n_bits, int sm_count, void* psi, void* lam,
+                   int batch, const void* bmat, int64_t bstride, double* gacc, int64_t gstride, int elem,
+                   cudaStream_t st) {
+  CUfunction f = static_cast<CUfunction>(m.afn[p]);
+  const PassDesc& pd = s.passes[p];
+  const int threads = 1 << (pd.t - s.reg_bits);
+  const size_t smem = jit_adj_smem(s, p, elem);
+  int per_sm = 0;
+  g_drv.occupancy(&per_sm, f, threads, smem);
+  if (per_sm < 1) per_sm = 1;
+  const int64_t ntiles = (1LL << (n_bits - pd.t)) * batch;
+  const int64_t cap = static_cast<int64_t>(sm_count) * per_sm;
+  const unsigned grid = static_cast<unsigned>(std::max<int64_t>(1, std::min(ntiles, cap)));
+  long long bs = bstride, gs = gstride;
+  const int32_t* mc = static_cast<const int32_t*>(m.mc) + m.mc_off[p];
+  const int32_t* gt = static_cast<const int32_t*>(m.gt) + m.gt_off[p];
+  void* args[] = {&psi, &lam, &batch, const_cast<void**>(&bmat), &bs, &mc, &gacc, &gs, &gt};
+  if (g_drv.launch(f, grid, 1, 1, threads, 1, 1, static_cast<unsigned>(smem), reinterpret_cast<CUstream>(st), args,
+                   nullptr) != CUDA_SUCCESS) {
+    set_error("cuLaunchKernel failed for a specialised adjoint pass");
     return JQ_ECUDA;
   }
   return JQ_OK;

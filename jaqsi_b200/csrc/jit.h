@@ -13,9 +13,13 @@ namespace jq {
 struct JitModule {
   void* module = nullptr;       // CUmodule
   std::vector<void*> fn;        // CUfunction per pass (nullptr: interpreter)
+  std::vector<void*> afn;       // adjoint CUfunction per pass (unitary statevector plans)
   void* mc = nullptr;           // device int32 matrix staging tables
+  void* gt = nullptr;           // device int32 gradient flush tables (adjoint)
   std::vector<int64_t> mc_off;  // per pass offset into mc
+  std::vector<int64_t> gt_off;  // per pass offset into gt
   int n_kernels = 0;            // distinct kernels after sharing identical passes
+  bool has_adjoint = false;
 };
 
 bool jit_available();
@@ -26,5 +30,13 @@ void jit_free(JitModule* m);
 size_t jit_smem(const Schedule& s, int p, int elem);
 int jit_launch(const JitModule& m, const Schedule& s, int p, int n_bits, int sm_count, void* state, int batch,
                const void* bmat, int64_t bstride, int elem, cudaStream_t st);
+
+size_t jit_adj_smem(const Schedule& s, int p, int elem);
+// One adjoint pass: psi <- G^dagger psi, lam <- G^dagger lam over the pass's
+// blocks in reverse; block cotangents into gacc (instance stride gstride
+// complex128 entries), none when gacc is NULL.
+int jit_launch_adj(const JitModule& m, const Schedule& s, int p, int n_bits, int sm_count, void* psi, void* lam,
+                   int batch, const void* bmat, int64_t bstride, double* gacc, int64_t gstride, int elem,
+                   cudaStream_t st);
 
 }  // namespace jq

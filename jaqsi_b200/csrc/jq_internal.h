@@ -108,7 +108,8 @@ struct RegOp {
   // w3: matrix offset in the block-matrix buffer (complex elements)
   uint32_t w0, w1, w2, w3;
   int32_t mat_len;     // complex elements of the matrix / diagonal (0: none)
-  int32_t pad[3];
+  int32_t grad_off;    // block cotangent accumulator (complex128 offset), -1 if none
+  int32_t pad[2];
 };
 
 constexpr int kMaxRegBits = 5;

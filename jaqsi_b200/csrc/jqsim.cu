@@ -2060,8 +2060,25 @@ int adjoint_impl(const jq_plan* plan, int batch, const double* angles, const voi
   if ((rc = seed_sv<R>(plan, T, batch, out_type, psi, ct, ct_state, lam, st))) return rc;
   const bool want_grad = (grad_angles || grad_mats) && plan->grad_stride > 0;
   if (want_grad) JQ_CUDA(cudaMemsetAsync(gacc, 0, 16 * static_cast<size_t>(plan->grad_stride) * batch, st));
+  // Specialised adjoint: the forward schedule's passes in reverse, each one
+  // kernel holding both tiles (psi and lam) in shared memory.
+  const JitModule* jm = static_cast<const JitModule*>(T->jit);
+  bool use_jit = jm && jm->has_adjoint;
+  if (use_jit)
+    for (size_t p = 0; p < plan->fwd.passes.size(); ++p)
+      if (plan->fwd.passes[p].op_end > plan->fwd.passes[p].op_begin && !jm->afn[p]) use_jit = false;
+  if (use_jit) {
+    const Schedule& fs = plan->fwd;
+    for (size_t pi = fs.passes.size(); pi-- > 0;) {
+      if (fs.passes[pi].op_end == fs.passes[pi].op_begin) continue;
+      if ((rc = jit_launch_adj(*jm, fs, static_cast<int>(pi), plan->n_bits, sm_count(), psi, lam, batch, bmat,
+                               plan->bmat_stride, want_grad ? reinterpret_cast<double*>(gacc) : nullptr,
+                               plan->grad_stride, static_cast<int>(sizeof(C)), st)))
+        return rc;
+    }
+  }
   const Schedule& sch = plan->adj;
-  for (size_t pi = sch.passes.size(); pi-- > 0;) {
+  for (size_t pi = sch.passes.size(); !use_jit && pi-- > 0;) {
     const PassDesc& pd = sch.passes[pi];
     if (pd.op_end == pd.op_begin) continue;
     const size_t smem = tile_smem<R>(pd, 2);

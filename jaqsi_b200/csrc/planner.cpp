@@ -349,6 +349,7 @@ void build_steps(Schedule& s, const std::vector<int32_t>& perm_pool, int dtype) 
         ro.w2 = static_cast<uint32_t>(smat);
         ro.w3 = static_cast<uint32_t>(op.mat_off < 0 ? 0 : op.mat_off);
         ro.mat_len = mat_len;
+        ro.grad_off = (kind == RK_PERM1 || kind == RK_PERM2) ? -1 : op.grad_off;
         smat += mat_len;
         s.rops.push_back(ro);
       }

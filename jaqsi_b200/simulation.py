@@ -334,6 +334,45 @@ def get_plan(lw: Lowered, obs_specs, obs_key, n_qubits: int, mode: int, dtype: t
     return plan
 
 
+def _view_gather(values: list, device: torch.device) -> Optional[torch.Tensor]:
+    """One index op when every tensor angle is a one-element view of the same
+    contiguous base tensor (the ``params[l, w, i]`` pattern); None otherwise.
+
+    The views the circuit created are bypassed: gradients reach the base
+    through a single scatter instead of one select-backward per angle.
+    """
+    base = None
+    pos, offs, fpos, fval = [], [], [], []
+    for i, v in enumerate(values):
+        if isinstance(v, torch.Tensor):
+            b = v._base
+            if b is None or v.numel() != 1 or v.dtype != b.dtype or not b.is_floating_point():
+                return None
+            if base is None:
+                base = b
+                if not base.is_contiguous():
+                    return None
+            elif b is not base:
+                return None
+            pos.append(i)
+            offs.append(v.storage_offset() - base.storage_offset())
+        else:
+            fpos.append(i)
+            fval.append(float(v))
+    if base is None:
+        return None
+    flat = base.reshape(-1)
+    idx = torch.tensor(offs, dtype=torch.long).to(flat.device, non_blocking=True)
+    vals = flat.index_select(0, idx).to(torch.float64)
+    if not fpos:
+        return vals.to(device)
+    full = torch.zeros(len(values), dtype=torch.float64)
+    full[fpos] = torch.tensor(fval, dtype=torch.float64)
+    full = full.to(vals.device)
+    out = full.index_copy(0, torch.tensor(pos, dtype=torch.long).to(vals.device), vals)
+    return out.to(device)
+
+
 def gather_angles(values: list, device: torch.device) -> Optional[torch.Tensor]:
     """One float64 device tensor of the tape's angles (keeps autograd links)."""
     if not values:
@@ -341,6 +380,9 @@ def gather_angles(values: list, device: torch.device) -> Optional[torch.Tensor]:
     tensors = [v for v in values if isinstance(v, torch.Tensor)]
     if not tensors:
         return torch.tensor([float(v) for v in values], dtype=torch.float64).to(device, non_blocking=True)
+    fast = _view_gather(values, device)
+    if fast is not None:
+        return fast
     devs = {t.device for t in tensors}
     home = tensors[0].device if len(devs) == 1 else device
     parts = [

@@ -154,3 +154,31 @@ def test_pauli_detection():
     specs, _ = sim._lower_obs([jq.build_parity_observable([0, 2]), jq.PauliX(1)], 3)
     assert specs[0][:5] == ("P", 0, 0b101, 0, 1.0)
     assert specs[1][:5] == ("P", 0b010, 0, 0, 1.0)
+
+
+def test_view_gather_matches_stack_and_gradient():
+    """Angles that are element views of one tensor are gathered with one index
+    op; values and gradients equal the per-angle stack."""
+    base = torch.tensor(np.random.default_rng(0).uniform(0, 6, (4, 3, 3)), requires_grad=True)
+
+    def circuit(a):
+        for l in range(4):
+            for w in range(3):
+                jq.Rot(a[l, w, 0], a[l, w, 1], a[l, w, 2], wires=w)
+            jq.RX(0.25, wires=0)
+            jq.CX(wires=[0, 2])
+
+    tape = jq.Script(circuit, 3).record(base)
+    lw = sim.lower_tape(tape, 3)
+    fast = sim._view_gather(lw.angles, torch.device("cpu"))
+    assert fast is not None
+    ref = torch.stack([v.double().reshape(()) if isinstance(v, torch.Tensor) else torch.tensor(float(v),
+                       dtype=torch.float64) for v in lw.angles])
+    assert torch.equal(fast, ref)
+    w = torch.randn(ref.shape, dtype=torch.float64)
+    g1, = torch.autograd.grad((fast * w).sum(), base)
+    g2, = torch.autograd.grad((ref * w).sum(), base)
+    assert torch.allclose(g1, g2)
+    # views of different tensors fall back to the stack
+    other = torch.zeros(2, requires_grad=True)
+    assert sim._view_gather([base[0, 0, 0], other[1]], torch.device("cpu")) is None
