@@ -346,7 +346,8 @@ def ours_arm(args):
         "config": _config(args, p_ref, P),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
-                     "kernel": "k_tile_fwd", "launches_per_step": P,
+                     "kernel": "jqk* (tile pass specialised per plan by NVRTC)",
+                     "launches_per_step": P,
                      "avg_launch_us": sweep_ms * 1e3 / P, "bytes_per_launch": pass_bytes},
         "e2e": {"value": e2e_value, "unit": "GB/s", "ms_per_step": e2e_ms,
                 "h2d_bytes_per_step": int(plan.n_angles * 8), "d2h_bytes_per_step": int(plan.n_obs * elem // 2)},

@@ -18,6 +18,7 @@
 #include <nvrtc.h>
 
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <sstream>
@@ -106,8 +107,83 @@ __device__ __forceinline__ u64 pdep64(u64 v, u64 mask) {
   for (u64 bb = 1; mask; bb <<= 1) { u64 low = mask & (~mask + 1); if (v & bb) r |= low; mask &= mask - 1; }
   return r;
 }
+__device__ __forceinline__ void cp_async8(void* s, const void* g) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(s);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(g) : "memory");
+}
+__device__ __forceinline__ void cp_async16(void* s, const void* g) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(s);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(g) : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 __device__ __forceinline__ u32 swz8(u32 l) { return l ^ (((l >> 4) ^ (l >> 8) ^ (l >> 12)) & 15u); }
 __device__ __forceinline__ u32 swz16(u32 l) { return l ^ (((l >> 3) ^ (l >> 6) ^ (l >> 9) ^ (l >> 12)) & 7u); }
+// Asynchronous tile load (global -> swizzled shared memory, no registers):
+// one 8-byte (complex64) or 16-byte (complex128) copy per amplitude.
+__device__ __forceinline__ void prefetch8(float2* s, const float2* g, const u32* tbl, int t, int c) {
+  const int cm = (1 << c) - 1, nv = 1 << t;
+  for (int l = threadIdx.x; l < nv; l += blockDim.x) cp_async8(s + swz8(l), g + (tbl[l >> c] | (l & cm)));
+}
+__device__ __forceinline__ void prefetch16(double2* s, const double2* g, const u32* tbl, int t, int c) {
+  const int cm = (1 << c) - 1, nv = 1 << t;
+  for (int l = threadIdx.x; l < nv; l += blockDim.x) cp_async16(s + swz16(l), g + (tbl[l >> c] | (l & cm)));
+}
+// Tile copies with the thread count (2^LT), tile bits TB and contiguous low
+// bits CB known at compile time.  Amplitude l = tid | (i << LT); the swizzle
+// is XOR-linear, so swz(l) = swz(tid) ^ swz(i << LT) with the second term a
+// constant; likewise l >> CB = (tid >> CB) | ((i << LT) >> CB) and
+// l & cm = (tid & cm) | ((i << LT) & cm) split into a per-thread and a constant part.
+template <int LT, int TB, int CB>
+__device__ __forceinline__ void prefetch8t(float2* s, const float2* g, const u32* tbl) {
+  constexpr u32 cm = (1u << CB) - 1u;
+  const u32 tid = threadIdx.x, st = swz8(tid), lo = tid & cm;
+  const u32* tb = tbl + (tid >> CB);
+#pragma unroll
+  for (int i = 0; i < (1 << (TB - LT)); ++i) {
+    const u32 hi = (u32)i << LT;
+    cp_async8(s + (st ^ swz8(hi)), g + (tb[hi >> CB] | lo | (hi & cm)));
+  }
+}
+template <int LT, int TB, int CB>
+__device__ __forceinline__ void prefetch16t(double2* s, const double2* g, const u32* tbl) {
+  constexpr u32 cm = (1u << CB) - 1u;
+  const u32 tid = threadIdx.x, st = swz16(tid), lo = tid & cm;
+  const u32* tb = tbl + (tid >> CB);
+#pragma unroll
+  for (int i = 0; i < (1 << (TB - LT)); ++i) {
+    const u32 hi = (u32)i << LT;
+    cp_async16(s + (st ^ swz16(hi)), g + (tb[hi >> CB] | lo | (hi & cm)));
+  }
+}
+// complex64 store: pairs (2v, 2v + 1), v = tid | (i << LT), one 16-byte store
+// each (CB >= 1: the pair is contiguous in global memory)
+template <int LT, int TB, int CB>
+__device__ __forceinline__ void store8t(const float2* s, float2* g, const u32* tbl) {
+  static_assert(CB >= 1, "complex64 pairs need one contiguous low bit");
+  constexpr u32 cm = (1u << CB) - 1u;
+  const u32 tid = threadIdx.x, l0 = 2 * tid, s0 = swz8(l0), s1 = swz8(l0 + 1), lo = l0 & cm;
+  const u32* tb = tbl + (l0 >> CB);
+#pragma unroll
+  for (int i = 0; i < (1 << (TB - 1 - LT)); ++i) {
+    const u32 hi = (u32)i << (LT + 1);
+    const u32 k = swz8(hi);
+    const float2 a = s[s0 ^ k], b = s[s1 ^ k];
+    __stcs((float4*)(g + (tb[hi >> CB] | lo | (hi & cm))), make_float4(a.x, a.y, b.x, b.y));
+  }
+}
+template <int LT, int TB, int CB>
+__device__ __forceinline__ void store16t(const double2* s, double2* g, const u32* tbl) {
+  constexpr u32 cm = (1u << CB) - 1u;
+  const u32 tid = threadIdx.x, st = swz16(tid), lo = tid & cm;
+  const u32* tb = tbl + (tid >> CB);
+#pragma unroll
+  for (int i = 0; i < (1 << (TB - LT)); ++i) {
+    const u32 hi = (u32)i << LT;
+    __stcs(g + (tb[hi >> CB] | lo | (hi & cm)), s[st ^ swz16(hi)]);
+  }
+}
+__device__ __forceinline__ void cp_wait0() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 template <int B>
 __device__ __forceinline__ void load8(float2* s, const float2* g, const u32* tbl, int t, int c) {
   const int cm = (1 << c) - 1, nv = (1 << t) / 2;
@@ -182,6 +258,37 @@ template <int N, typename F> __device__ __forceinline__ void warp_rs_add(F (&v)[
   constexpr int lg = (N >= 32) ? 5 : (N >= 16) ? 4 : (N >= 8) ? 3 : (N >= 4) ? 2 : (N >= 2) ? 1 : 0;
   if ((lane & ((32u >> lg) - 1u)) == 0) atomicAdd(dst + (lane >> (5 - lg)), (double)v[0]);
 }
+// Packed-float32 complex dot products (sm_100 two-lane FMA): with the matrix
+// entries staged as broadcast pairs (re, re) and (im, im),
+//   p = sum_q Re(m_q) (x_q.re, x_q.im),  s = sum_q Im(m_q) (x_q.re, x_q.im),
+//   sum_q m_q x_q = (p.re - s.im, p.im + s.re).
+__device__ __forceinline__ float2 cdot2(float2 ar, float2 ai, float2 br, float2 bi, float2 x, float2 y) {
+  float2 p = __fmul2_rn(ar, x), q = __fmul2_rn(ai, x);
+  p = __ffma2_rn(br, y, p);
+  q = __ffma2_rn(bi, y, q);
+  return make_float2(p.x - q.y, p.y + q.x);
+}
+__device__ __forceinline__ float2 lo2(float4 v) { return make_float2(v.x, v.y); }
+__device__ __forceinline__ float2 hi2(float4 v) { return make_float2(v.z, v.w); }
+// mb: one float4 (re, re, im, im) per matrix entry (one 16-byte shared load each)
+__device__ __forceinline__ float2 cdot4(const float4* mb, float2 a0, float2 a1, float2 a2, float2 a3) {
+  const float4 m0 = mb[0], m1 = mb[1], m2 = mb[2], m3 = mb[3];
+  float2 p = __fmul2_rn(lo2(m0), a0), q = __fmul2_rn(hi2(m0), a0);
+  p = __ffma2_rn(lo2(m1), a1, p);
+  q = __ffma2_rn(hi2(m1), a1, q);
+  p = __ffma2_rn(lo2(m2), a2, p);
+  q = __ffma2_rn(hi2(m2), a2, q);
+  p = __ffma2_rn(lo2(m3), a3, p);
+  q = __ffma2_rn(hi2(m3), a3, q);
+  return make_float2(p.x - q.y, p.y + q.x);
+}
+// sum_q conj(m_q) x_q from the same broadcast pairs
+__device__ __forceinline__ float2 cdot2c(float2 ar, float2 ai, float2 br, float2 bi, float2 x, float2 y) {
+  float2 p = __fmul2_rn(ar, x), q = __fmul2_rn(ai, x);
+  p = __ffma2_rn(br, y, p);
+  q = __ffma2_rn(bi, y, q);
+  return make_float2(p.x + q.y, p.y - q.x);
+}
 template <typename C> __device__ __forceinline__ C cconj(C a) { a.y = -a.y; return a; }
 // a * conj(b)
 template <typename C> __device__ __forceinline__ C cmulc(C a, C b) {
@@ -197,6 +304,25 @@ std::string hex(uint64_t v) {
 }
 
 // Emit the kernel of pass p (register-stage program only).
+// Straight-line bit deposit of `v` into the set bits of `mask`: one
+// shift-and-mask term per contiguous run of mask bits.
+std::string pdep_expr(const std::string& v, uint64_t mask) {
+  std::string e;
+  int src = 0;
+  for (int b = 0; b < 64;) {
+    if (!((mask >> b) & 1)) { ++b; continue; }
+    int len = 0;
+    while (b + len < 64 && ((mask >> (b + len)) & 1)) ++len;
+    const uint64_t lm = (len >= 64) ? ~0ULL : ((1ULL << len) - 1);
+    std::string term = "(((" + v + ") >> " + std::to_string(src) + ") & " + hex(lm) + ")";
+    if (b) term = "(" + term + " << " + std::to_string(b) + ")";
+    e += (e.empty() ? "" : " | ") + term;
+    src += len;
+    b += len;
+  }
+  return e.empty() ? std::string("0ull") : "(" + e + ")";
+}
+
 void emit_pass(std::ostringstream& o, const jq_plan* plan, const Schedule& s, int p, bool c64, int rb) {
   const PassDesc& pd = s.passes[p];
   const char* T = c64 ? "float2" : "double2";
@@ -205,7 +331,8 @@ void emit_pass(std::ostringstream& o, const jq_plan* plan, const Schedule& s, in
   const int nr = 1 << rb;
   // register budget: 16 complex64 amplitudes + a 4x4 matrix fit 128 registers;
   // complex128 needs about 168
-  const int minb = std::max(1, std::min(8, 65536 / (nthr * (c64 ? 128 : 168))));
+  int minb = std::max(1, std::min(8, 65536 / (nthr * (c64 ? 128 : 168))));
+  if (const char* e = std::getenv("JQ_JIT_MINB")) minb = std::max(1, std::min(16, std::atoi(e)));
   const uint64_t full = (nb >= 64) ? ~0ULL : ((1ULL << nb) - 1);
   const uint64_t outer = full & ~pd.tile_mask;
   const int smat_pad = (pd.smat_len + 1) & ~1;
@@ -214,10 +341,18 @@ void emit_pass(std::ostringstream& o, const jq_plan* plan, const Schedule& s, in
   o << "extern \"C\" __global__ void __launch_bounds__(" << nthr << ", " << minb << ") @KERNEL@(" << T
     << "* __restrict__ state, int batch, const " << T << "* __restrict__ bmat, long long bstride, "
     << "const int* __restrict__ mc) {\n";
+  // two tile buffers: the next tile streams in (cp.async) while this one is computed
   o << "  extern __shared__ __align__(16) unsigned char smem[];\n";
-  o << "  " << T << "* s = (" << T << "*)smem;\n";
-  o << "  " << T << "* smat = s + " << (1 << t) << ";\n";
-  o << "  u32* tbl = (u32*)(smat + " << smat_pad << ");\n";
+  o << "  " << T << "* s0 = (" << T << "*)smem;\n";
+  o << "  " << T << "* s1 = s0 + " << (1 << t) << ";\n";
+  o << "  " << T << "* smat = s1 + " << (1 << t) << ";\n";
+  if (c64) {
+    // broadcast copies (re, re), (im, im) of every staged matrix entry
+    o << "  float2* smatb = smat + " << smat_pad << ";\n";
+    o << "  u32* tbl = (u32*)(smatb + " << 2 * smat_pad << ");\n";
+  } else {
+    o << "  u32* tbl = (u32*)(smat + " << smat_pad << ");\n";
+  }
   o << "  const u32 tid = threadIdx.x;\n";
   // bit-deposit table of the tile's high bits
   o << "  { const u32 hb[] = {";
@@ -234,21 +369,34 @@ void emit_pass(std::ostringstream& o, const jq_plan* plan, const Schedule& s, in
     o << "\n";
     ++nstage;
   }
+  const std::string tpl = "<" + std::to_string(t - rb) + ", " + std::to_string(t) + ", " + std::to_string(c) + ">";
+  const std::string pf = (c64 ? "prefetch8t" : "prefetch16t") + tpl;
   o << "  const long long tiles_per = 1ll << " << (nb - t) << ";\n";
   o << "  const long long ntiles = tiles_per * batch;\n";
+  o << "  auto gaddr = [&](long long tl) { const u64 ti = (u64)tl & (u64)(tiles_per - 1); return state + ((tl >> "
+    << (nb - t) << ") << " << nb << ") + " << pdep_expr("ti", outer) << "; };\n";
+  o << "  __syncthreads();\n";
+  o << "  if ((long long)blockIdx.x < ntiles) " << pf << "(s0, gaddr(blockIdx.x), tbl);\n";
+  o << "  cp_commit();\n";
   o << "  long long last_inst = -1;\n";
-  o << "  for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {\n";
+  o << "  int kk = 0;\n";
+  o << "  for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++kk) {\n";
+  o << "    " << T << "* s = (kk & 1) ? s1 : s0;\n";
+  o << "    if (tile + gridDim.x < ntiles) " << pf << "((kk & 1) ? s0 : s1, gaddr(tile + gridDim.x), tbl);\n";
+  o << "    cp_commit();\n";
   o << "    const long long inst = tile >> " << (nb - t) << ";\n";
-  o << "    const u64 ti = (u64)tile & (u64)(tiles_per - 1);\n";
-  o << "    " << T << "* g = state + (inst << " << nb << ") + pdep64(ti, " << hex(outer) << ");\n";
-  o << "    __syncthreads();\n";
+  o << "    " << T << "* g = gaddr(tile);\n";
   // gate matrices of this pass: mc holds (smem offset, block-matrix offset,
   // length) per matrix, so passes that differ only in their gates share code
   o << "    if (inst != last_inst) {\n      const " << T << "* bm = bmat + inst * bstride;\n";
   o << "      for (int i = 0; i < " << nmc << "; ++i) { const int d = mc[3 * i], a = mc[3 * i + 1], n = mc[3 * i + 2];\n";
-  o << "        for (int e = tid; e < n; e += blockDim.x) smat[d + e] = bm[a + e]; }\n";
+  if (c64)
+    o << "        for (int e = tid; e < n; e += blockDim.x) { const float2 v = bm[a + e]; smat[d + e] = v; "
+         "smatb[2 * (d + e)] = make_float2(v.x, v.x); smatb[2 * (d + e) + 1] = make_float2(v.y, v.y); } }\n";
+  else
+    o << "        for (int e = tid; e < n; e += blockDim.x) smat[d + e] = bm[a + e]; }\n";
   o << "      (void)bm; last_inst = inst;\n    }\n";
-  o << "    " << (c64 ? "load8<4>" : "load16<2>") << "(s, g, tbl, " << t << ", " << c << ");\n";
+  o << "    cp_wait1();\n";
   o << "    __syncthreads();\n";
   nstage = 0;
   for (int si = pd.step_begin; si < pd.step_end; ++si) {
@@ -275,7 +423,19 @@ void emit_pass(std::ostringstream& o, const jq_plan* plan, const Schedule& s, in
       if (guard) o << "      if ((tid & " << ctm << "u) == " << ctm << "u) {\n";
       else o << "      {\n";
       auto V = [&](int j) { return std::string("v") + std::to_string(var[j]); };
-      if (kind == RK_DENSE1) {
+      if (kind == RK_DENSE1 && c64) {
+        o << "        const float4* mq = (const float4*)smatb + " << M << ";\n";
+        o << "        const float4 A = mq[0], Bq = mq[1], Cq = mq[2], Dq = mq[3];\n";
+        o << "        const float2 ar = lo2(A), ai = hi2(A), br = lo2(Bq), bi = hi2(Bq), cr = lo2(Cq), ci = hi2(Cq), "
+             "dr = lo2(Dq), di = hi2(Dq);\n";
+        for (int j = 0; j < nr; ++j) {
+          if ((j >> q1) & 1) continue;
+          if ((static_cast<uint32_t>(j) & crm) != crm) continue;
+          const int k = j | (1 << q1);
+          o << "        { const float2 x = " << V(j) << ", y = " << V(k) << "; " << V(j)
+            << " = cdot2(ar, ai, br, bi, x, y); " << V(k) << " = cdot2(cr, ci, dr, di, x, y); }\n";
+        }
+      } else if (kind == RK_DENSE1) {
         o << "        const " << T << " m00 = smat[" << M << "], m01 = smat[" << M + 1 << "], m10 = smat[" << M + 2
           << "], m11 = smat[" << M + 3 << "];\n";
         for (int j = 0; j < nr; ++j) {
@@ -303,6 +463,17 @@ void emit_pass(std::ostringstream& o, const jq_plan* plan, const Schedule& s, in
           int idx = 0;
           for (uint32_t i = 0; i < dk; ++i) idx = (idx << 1) | ((j >> ((dq >> (3 * i)) & 7u)) & 1);
           o << "        " << V(j) << " = cmul(smat[" << M + idx << "], " << V(j) << ");\n";
+        }
+      } else if (kind == RK_DENSE2 && c64) {
+        for (int j = 0; j < nr; ++j) {
+          if (((j >> q1) & 1) || ((j >> q2) & 1)) continue;
+          if ((static_cast<uint32_t>(j) & crm) != crm) continue;
+          const int id[4] = {j, j | (1 << q2), j | (1 << q1), j | (1 << q1) | (1 << q2)};
+          o << "        { const float2 a0 = " << V(id[0]) << ", a1 = " << V(id[1]) << ", a2 = " << V(id[2])
+            << ", a3 = " << V(id[3]) << ";\n";
+          for (int r = 0; r < 4; ++r)
+            o << "          " << V(id[r]) << " = cdot4((const float4*)smatb + " << M + 4 * r << ", a0, a1, a2, a3);\n";
+          o << "        }\n";
         }
       } else if (kind == RK_DENSE2) {
         o << "        " << T << " mm[16];\n        for (int e = 0; e < 16; ++e) mm[e] = smat[" << M << " + e];\n";
@@ -342,7 +513,8 @@ void emit_pass(std::ostringstream& o, const jq_plan* plan, const Schedule& s, in
     o << "    }\n    __syncthreads();\n";
     ++nstage;
   }
-  o << "    " << (c64 ? "store8<4>" : "store16<2>") << "(s, g, tbl, " << t << ", " << c << ");\n";
+  o << "    " << (c64 ? "store8t" : "store16t") << tpl << "(s, g, tbl);\n";
+  o << "    __syncthreads();\n";
   o << "  }\n}\n";
 }
 
@@ -381,7 +553,12 @@ void emit_adj_pass(std::ostringstream& o, const jq_plan* plan, const Schedule& s
   o << "  " << T << "* sp = (" << T << "*)smem;\n";
   o << "  " << T << "* sl = sp + " << (1 << t) << ";\n";
   o << "  " << T << "* smat = sl + " << (1 << t) << ";\n";
-  o << "  double* sacc = (double*)(smat + " << smat_pad << ");\n";
+  if (c64) {
+    o << "  float2* smatb = smat + " << smat_pad << ";\n";
+    o << "  double* sacc = (double*)(smatb + " << 2 * smat_pad << ");\n";
+  } else {
+    o << "  double* sacc = (double*)(smat + " << smat_pad << ");\n";
+  }
   o << "  u32* tbl = (u32*)(sacc + " << nacc_pad << ");\n";
   o << "  const u32 tid = threadIdx.x;\n";
   o << "  { const u32 hb[] = {";
@@ -412,17 +589,23 @@ void emit_adj_pass(std::ostringstream& o, const jq_plan* plan, const Schedule& s
   o << "  for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {\n";
   o << "    const long long inst = tile >> " << (nb - t) << ";\n";
   o << "    const u64 ti = (u64)tile & (u64)(tiles_per - 1);\n";
-  o << "    const long long goff = (inst << " << nb << ") + (long long)pdep64(ti, " << hex(outer) << ");\n";
+  o << "    const long long goff = (inst << " << nb << ") + (long long)" << pdep_expr("ti", outer) << ";\n";
   o << "    __syncthreads();\n";
   o << "    if (inst != last_inst) {\n";
   o << "      if (last_inst >= 0) {\n" << flush_for("last_inst") << "        __syncthreads();\n";
   o << "        for (int e = tid; e < " << nacc_pad << "; e += blockDim.x) sacc[e] = 0.0;\n      }\n";
   o << "      const " << T << "* bm = bmat + inst * bstride;\n";
   o << "      for (int i = 0; i < " << nmc << "; ++i) { const int d = mc[3 * i], a = mc[3 * i + 1], n = mc[3 * i + 2];\n";
-  o << "        for (int e = tid; e < n; e += blockDim.x) smat[d + e] = bm[a + e]; }\n";
+  if (c64)
+    o << "        for (int e = tid; e < n; e += blockDim.x) { const float2 v = bm[a + e]; smat[d + e] = v; "
+         "smatb[2 * (d + e)] = make_float2(v.x, v.x); smatb[2 * (d + e) + 1] = make_float2(v.y, v.y); } }\n";
+  else
+    o << "        for (int e = tid; e < n; e += blockDim.x) smat[d + e] = bm[a + e]; }\n";
   o << "      (void)bm; last_inst = inst;\n      __syncthreads();\n    }\n";
-  o << "    " << (c64 ? "load8<4>" : "load16<2>") << "(sp, psi + goff, tbl, " << t << ", " << c << ");\n";
-  o << "    " << (c64 ? "load8<4>" : "load16<2>") << "(sl, lam + goff, tbl, " << t << ", " << c << ");\n";
+  const std::string tpl = "<" + std::to_string(t - rb) + ", " + std::to_string(t) + ", " + std::to_string(c) + ">";
+  o << "    " << (c64 ? "prefetch8t" : "prefetch16t") << tpl << "(sp, psi + goff, tbl);\n";
+  o << "    " << (c64 ? "prefetch8t" : "prefetch16t") << tpl << "(sl, lam + goff, tbl);\n";
+  o << "    cp_commit();\n    cp_wait0();\n";
   o << "    __syncthreads();\n";
   for (int si = pd.step_end - 1; si >= pd.step_begin; --si) {
     const int k = si - pd.step_begin;
@@ -461,22 +644,32 @@ void emit_adj_pass(std::ostringstream& o, const jq_plan* plan, const Schedule& s
       }
       if (guard) o << "        if ((tid & " << ctm << "u) == " << ctm << "u) {\n";
       else o << "        {\n";
+      auto B = [&](uint32_t e, int part) { return "smatb[" + std::to_string(2 * (M + e) + part) + "]"; };
       if (kind == RK_DENSE1) {
         // G^dagger = [[conj m00, conj m10], [conj m01, conj m11]]
-        o << "          const " << T << " h00 = cconj(smat[" << M << "]), h01 = cconj(smat[" << M + 2
-          << "]), h10 = cconj(smat[" << M + 1 << "]), h11 = cconj(smat[" << M + 3 << "]);\n";
+        if (c64)
+          o << "          const float4* mq = (const float4*)smatb + " << M << ";\n"
+            << "          const float4 A = mq[0], Bq = mq[2], Cq = mq[1], Dq = mq[3];\n"
+            << "          const float2 ar = lo2(A), ai = hi2(A), br = lo2(Bq), bi = hi2(Bq), cr = lo2(Cq), ci = hi2(Cq), "
+               "dr = lo2(Dq), di = hi2(Dq);\n";
+        else
+          o << "          const " << T << " h00 = cconj(smat[" << M << "]), h01 = cconj(smat[" << M + 2
+            << "]), h10 = cconj(smat[" << M + 1 << "]), h11 = cconj(smat[" << M + 3 << "]);\n";
+        auto upd = [&](const std::string& a, const std::string& b) {
+          if (c64)
+            return a + " = cdot2c(ar, ai, br, bi, x, y); " + b + " = cdot2c(cr, ci, dr, di, x, y);";
+          return a + " = cfma(h01, y, cmul(h00, x)); " + b + " = cfma(h11, y, cmul(h10, x));";
+        };
         for (int j = 0; j < nr; ++j) {
           if ((j >> q1) & 1) continue;
           if ((static_cast<uint32_t>(j) & crm) != crm) continue;
           const int kk = j | (1 << q1);
-          o << "          { const " << T << " x = " << P(j) << ", y = " << P(kk) << "; " << P(j)
-            << " = cfma(h01, y, cmul(h00, x)); " << P(kk) << " = cfma(h11, y, cmul(h10, x));\n";
+          o << "          { " << T << " x = " << P(j) << ", y = " << P(kk) << "; " << upd(P(j), P(kk)) << "\n";
           if (grad)
             o << "            g[0] = cadd(g[0], cmulc(" << Lm(j) << ", " << P(j) << ")); g[1] = cadd(g[1], cmulc(" << Lm(j)
               << ", " << P(kk) << ")); g[2] = cadd(g[2], cmulc(" << Lm(kk) << ", " << P(j)
               << ")); g[3] = cadd(g[3], cmulc(" << Lm(kk) << ", " << P(kk) << "));\n";
-          o << "            const " << T << " u = " << Lm(j) << ", w = " << Lm(kk) << "; " << Lm(j)
-            << " = cfma(h01, w, cmul(h00, u)); " << Lm(kk) << " = cfma(h11, w, cmul(h10, u)); }\n";
+          o << "            x = " << Lm(j) << "; y = " << Lm(kk) << "; " << upd(Lm(j), Lm(kk)) << " }\n";
         }
       } else if (kind == RK_PERM1) {
         for (int j = 0; j < nr; ++j) {
@@ -509,9 +702,23 @@ void emit_adj_pass(std::ostringstream& o, const jq_plan* plan, const Schedule& s
             << ", a3 = " << P(id[3]) << ";\n";
           // (G^dagger)[r][q] = conj(G[q][r]), read from shared memory each time
           auto H = [&](int r, int q) { return "cconj(smat[" + std::to_string(M + 4 * q + r) + "])"; };
-          for (int r = 0; r < 4; ++r)
+          // complex64: sum_q conj(G[q][r]) a_q from the broadcast pairs
+          auto HC = [&](const std::string& dst, int r, const char* a) {
+            std::string e = "{ float2 p = __fmul2_rn(" + B(r, 0) + ", " + a + "0), q = __fmul2_rn(" + B(r, 1) + ", " +
+                            a + "0);";
+            for (int q = 1; q < 4; ++q)
+              e += " p = __ffma2_rn(" + B(4 * q + r, 0) + ", " + a + std::to_string(q) + ", p); q = __ffma2_rn(" +
+                   B(4 * q + r, 1) + ", " + a + std::to_string(q) + ", q);";
+            return e + " " + dst + " = make_float2(p.x + q.y, p.y - q.x); }";
+          };
+          for (int r = 0; r < 4; ++r) {
+            if (c64) {
+              o << "            " << HC(P(id[r]), r, "a") << "\n";
+              continue;
+            }
             o << "            " << P(id[r]) << " = cfma(" << H(r, 3) << ", a3, cfma(" << H(r, 2) << ", a2, cfma("
               << H(r, 1) << ", a1, cmul(" << H(r, 0) << ", a0))));\n";
+          }
           if (grad)
             for (int r = 0; r < 4; ++r)
               for (int q = 0; q < 4; ++q)
@@ -519,9 +726,14 @@ void emit_adj_pass(std::ostringstream& o, const jq_plan* plan, const Schedule& s
                   << P(id[q]) << "));\n";
           o << "            const " << T << " b0 = " << Lm(id[0]) << ", b1 = " << Lm(id[1]) << ", b2 = " << Lm(id[2])
             << ", b3 = " << Lm(id[3]) << ";\n";
-          for (int r = 0; r < 4; ++r)
+          for (int r = 0; r < 4; ++r) {
+            if (c64) {
+              o << "            " << HC(Lm(id[r]), r, "b") << "\n";
+              continue;
+            }
             o << "            " << Lm(id[r]) << " = cfma(" << H(r, 3) << ", b3, cfma(" << H(r, 2) << ", b2, cfma("
               << H(r, 1) << ", b1, cmul(" << H(r, 0) << ", b0))));\n";
+          }
           o << "          }\n";
         }
       } else {  // RK_PERM2, inverse: new[p[r]] = old[r]
@@ -566,8 +778,8 @@ void emit_adj_pass(std::ostringstream& o, const jq_plan* plan, const Schedule& s
         << "u] = l" << var[j] << ";\n";
     o << "    }\n    __syncthreads();\n";
   }
-  o << "    " << (c64 ? "store8<4>" : "store16<2>") << "(sp, psi + goff, tbl, " << t << ", " << c << ");\n";
-  o << "    " << (c64 ? "store8<4>" : "store16<2>") << "(sl, lam + goff, tbl, " << t << ", " << c << ");\n";
+  o << "    " << (c64 ? "store8t" : "store16t") << tpl << "(sp, psi + goff, tbl);\n";
+  o << "    " << (c64 ? "store8t" : "store16t") << tpl << "(sl, lam + goff, tbl);\n";
   o << "  }\n  __syncthreads();\n  if (last_inst >= 0) {\n" << flush_for("last_inst") << "  }\n}\n";
 }
 
@@ -747,7 +959,8 @@ void jit_free(JitModule* m) {
 
 size_t jit_smem(const Schedule& s, int p, int elem) {
   const PassDesc& pd = s.passes[p];
-  return (static_cast<size_t>(1) << pd.t) * elem + static_cast<size_t>((pd.smat_len + 1) & ~1) * elem +
+  const size_t smat_pad = static_cast<size_t>((pd.smat_len + 1) & ~1);
+  return 2 * (static_cast<size_t>(1) << pd.t) * elem + smat_pad * elem + (elem == 8 ? 2 * smat_pad * elem : 0) +
          (static_cast<size_t>(1) << (pd.t - pd.c)) * 4;
 }
 
@@ -783,7 +996,8 @@ size_t jit_adj_smem(const Schedule& s, int p, int elem) {
   int nacc = 0;
   for (int ri = pd.rop_begin; ri < pd.rop_end; ++ri)
     if (s.rops[ri].grad_off >= 0) nacc += 2 * s.rops[ri].mat_len;
-  return 2 * (static_cast<size_t>(1) << pd.t) * elem + static_cast<size_t>((pd.smat_len + 1) & ~1) * elem +
+  const size_t smat_pad = static_cast<size_t>((pd.smat_len + 1) & ~1);
+  return 2 * (static_cast<size_t>(1) << pd.t) * elem + smat_pad * elem + (elem == 8 ? 2 * smat_pad * elem : 0) +
          static_cast<size_t>((nacc + 1) & ~1) * 8 + (static_cast<size_t>(1) << (pd.t - pd.c)) * 4;
 }
 

@@ -78,19 +78,26 @@ __device__ __forceinline__ int target_index(int l, const TileOp& op) {
 }
 
 // Sum `nv` per-thread doubles over the CTA; thread v < nv receives total v.
-__device__ inline void block_reduce(double* vals, int nv, double* red) {
+// Block-wide sum of NV per-thread values; thread v < NV gets sum v in vals[0].
+// NV is a compile-time count so the values stay in registers.
+template <int NV>
+__device__ __forceinline__ void block_reduce(double (&vals)[NV], double* red) {
+  static_assert(NV <= kRedSlots, "reduction scratch too small");
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  for (int v = 0; v < nv; ++v) {
+#pragma unroll
+  for (int v = 0; v < NV; ++v) {
     double x = vals[v];
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
     vals[v] = x;
   }
   __syncthreads();
-  if (lane == 0)
-    for (int v = 0; v < nv; ++v) red[warp * kRedSlots + v] = vals[v];
+  if (lane == 0) {
+#pragma unroll
+    for (int v = 0; v < NV; ++v) red[warp * kRedSlots + v] = vals[v];
+  }
   __syncthreads();
-  if (threadIdx.x < nv) {
+  if (threadIdx.x < NV) {
     double s = 0.0;
     for (int w = 0; w < nw; ++w) s += red[w * kRedSlots + threadIdx.x];
     vals[0] = s;
@@ -788,7 +795,7 @@ __device__ void adj_dense(C* sp, C* sl, int t, const TileOp& op, const C* __rest
       vals[2 * e] = acc[e].x;
       vals[2 * e + 1] = acc[e].y;
     }
-    block_reduce(vals, 2 * D * D, red);
+    block_reduce<2 * D * D>(vals, red);
     if (threadIdx.x < 2 * D * D) atomicAdd(reinterpret_cast<double*>(gacc + op.grad_off) + threadIdx.x, vals[0]);
   }
 }
@@ -868,7 +875,7 @@ __device__ void adj_diag(C* sp, C* sl, int t, const TileOp& op, const C* __restr
       vals[2 * q] = acc[q].x;
       vals[2 * q + 1] = acc[q].y;
     }
-    block_reduce(vals, 2 * D, red);
+    block_reduce<8>(vals, red);
     if (threadIdx.x < 2 * D) atomicAdd(reinterpret_cast<double*>(gacc + op.grad_off) + threadIdx.x, vals[0]);
   }
 }
@@ -981,7 +988,7 @@ __device__ void bwd_dense(const C* sx, C* sl, int t, const TileOp& op, const C* 
       vals[2 * e] = acc[e].x;
       vals[2 * e + 1] = acc[e].y;
     }
-    block_reduce(vals, 2 * D * D, red);
+    block_reduce<2 * D * D>(vals, red);
     if (threadIdx.x < 2 * D * D) atomicAdd(reinterpret_cast<double*>(gacc + op.grad_off) + threadIdx.x, vals[0]);
   }
 }
@@ -1051,7 +1058,7 @@ __device__ void bwd_diag(const C* sx, C* sl, int t, const TileOp& op, const C* _
       vals[2 * q] = acc[q].x;
       vals[2 * q + 1] = acc[q].y;
     }
-    block_reduce(vals, 2 * D, red);
+    block_reduce<8>(vals, red);
     if (threadIdx.x < 2 * D) atomicAdd(reinterpret_cast<double*>(gacc + op.grad_off) + threadIdx.x, vals[0]);
   }
 }
@@ -1336,18 +1343,115 @@ __device__ __forceinline__ double2 mul_iy(int ny, double2 w) {
 constexpr int kObsChunk = 16;
 
 // <psi| coeff P |psi> for up to kObsChunk Pauli words, float64 accumulation.
+// Z strings only (x_mask == 0 for every word of the chunk), one read of the
+// state.  A thread takes 8 consecutive amplitudes j0 + u at a time and forms
+// the Walsh sums w[m] = sum_u (-1)^popc(u & m) |psi_{j0+u}|^2 (m < 8) in
+// shared memory; word z then adds (-1)^popc((j0 >> 3) & (z >> 3)) w[z & 7].
+// The coefficients multiply the reduced sums.  Needs z >> 3 < 2^32.
+template <typename C>
+__device__ __forceinline__ void probs8(const C* p, double pa[8]);
+template <>
+__device__ __forceinline__ void probs8<float2>(const float2* p, double pa[8]) {
+  const float4* q = reinterpret_cast<const float4*>(p);
+#pragma unroll
+  for (int h = 0; h < 4; ++h) {
+    const float4 v = q[h];
+    pa[2 * h] = static_cast<double>(v.x) * v.x + static_cast<double>(v.y) * v.y;
+    pa[2 * h + 1] = static_cast<double>(v.z) * v.z + static_cast<double>(v.w) * v.w;
+  }
+}
+template <>
+__device__ __forceinline__ void probs8<double2>(const double2* p, double pa[8]) {
+#pragma unroll
+  for (int u = 0; u < 8; ++u) {
+    const double2 v = p[u];
+    pa[u] = v.x * v.x + v.y * v.y;
+  }
+}
+
 template <typename R>
-__global__ void k_expval_pauli_sv(const typename CplxT<R>::T* psi, int64_t dim, const DevObs* obs, int o_begin,
-                                  int o_cnt, double* out, int n_obs) {
-  __shared__ double red[32 * kRedSlots];
+__global__ void __launch_bounds__(256, 2) k_expval_zdiag_sv(const typename CplxT<R>::T* psi, int64_t dim,
+                                                            const DevObs* obs, int o_begin, int o_cnt, double* out,
+                                                            int n_obs) {
+  __shared__ double red[8 * kRedSlots];
+  __shared__ double sw[8][256];
+  __shared__ uint2 sinfo[kObsChunk];
+  __shared__ double sc[kObsChunk];
+  const int tid = threadIdx.x;
+  if (tid < kObsChunk) {
+    const bool on = tid < o_cnt;
+    const DevObs ob = obs[o_begin + (on ? tid : 0)];
+    sinfo[tid] = make_uint2(static_cast<uint32_t>(ob.z_mask >> 3), static_cast<uint32_t>(ob.z_mask & 7));
+    sc[tid] = on ? ob.coeff : 0.0;
+  }
+  __syncthreads();
+  const int inst = blockIdx.y;
+  const auto* p = psi + static_cast<int64_t>(inst) * dim;
+  double acc[kObsChunk];
+#pragma unroll
+  for (int o = 0; o < kObsChunk; ++o) acc[o] = 0.0;
+  const int64_t ng = dim >> 3;
+  for (int64_t g = static_cast<int64_t>(blockIdx.x) * blockDim.x + tid; g < ng;
+       g += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    double pa[8];
+    probs8(p + (g << 3), pa);
+    const double a0 = pa[0] + pa[1], a1 = pa[0] - pa[1], a2 = pa[2] + pa[3], a3 = pa[2] - pa[3];
+    const double a4 = pa[4] + pa[5], a5 = pa[4] - pa[5], a6 = pa[6] + pa[7], a7 = pa[6] - pa[7];
+    const double b0 = a0 + a2, b1 = a1 + a3, b2 = a0 - a2, b3 = a1 - a3;
+    const double b4 = a4 + a6, b5 = a5 + a7, b6 = a4 - a6, b7 = a5 - a7;
+    sw[0][tid] = b0 + b4;
+    sw[1][tid] = b1 + b5;
+    sw[2][tid] = b2 + b6;
+    sw[3][tid] = b3 + b7;
+    sw[4][tid] = b0 - b4;
+    sw[5][tid] = b1 - b5;
+    sw[6][tid] = b2 - b6;
+    sw[7][tid] = b3 - b7;
+    const uint32_t gh = static_cast<uint32_t>(g);
+#pragma unroll
+    for (int o = 0; o < kObsChunk; ++o) {
+      if (o < o_cnt) {
+        // volatile: re-read per group instead of holding 2 x 16 words in registers
+        const volatile uint32_t* vi = reinterpret_cast<const volatile uint32_t*>(sinfo) + 2 * o;
+        const uint32_t zx = vi[0], zl = vi[1];
+        const double w = sw[zl][tid];
+        acc[o] += (__popc(gh & zx) & 1) ? -w : w;
+      }
+    }
+  }
+  // fewer than 8 amplitudes (up to two qubits)
+  if (dim < 8 && blockIdx.x == 0) {
+    for (int64_t j = tid; j < dim; j += blockDim.x) {
+      const double2 a = to_d2(p[j]);
+      const double pj = a.x * a.x + a.y * a.y;
+#pragma unroll
+      for (int o = 0; o < kObsChunk; ++o) {
+        if (o < o_cnt) {
+          const uint64_t z = (static_cast<uint64_t>(sinfo[o].x) << 3) | sinfo[o].y;
+          acc[o] += (__popcll(static_cast<uint64_t>(j) & z) & 1) ? -pj : pj;
+        }
+      }
+    }
+  }
+  block_reduce<kObsChunk>(acc, red);
+  if (tid < o_cnt) atomicAdd(&out[static_cast<int64_t>(inst) * n_obs + o_begin + tid], sc[tid] * acc[0]);
+}
+
+// General Pauli words: <psi| coeff P |psi> = coeff sum_j conj(psi_j) phase(j ^ x) psi_{j ^ x}.
+template <typename R>
+__global__ void __launch_bounds__(256, 2) k_expval_pauli_sv(const typename CplxT<R>::T* psi, int64_t dim,
+                                                            const DevObs* obs, int o_begin, int o_cnt, double* out,
+                                                            int n_obs) {
+  __shared__ double red[8 * kRedSlots];
   __shared__ uint64_t sx[kObsChunk], sz[kObsChunk];
   __shared__ double sc[kObsChunk];
   __shared__ int sy[kObsChunk];
-  if (threadIdx.x < o_cnt) {
-    const DevObs ob = obs[o_begin + threadIdx.x];
+  if (threadIdx.x < kObsChunk) {
+    const bool on = threadIdx.x < o_cnt;
+    const DevObs ob = obs[o_begin + (on ? threadIdx.x : 0)];
     sx[threadIdx.x] = ob.x_mask;
     sz[threadIdx.x] = ob.z_mask;
-    sc[threadIdx.x] = ob.coeff;
+    sc[threadIdx.x] = on ? ob.coeff : 0.0;
     sy[threadIdx.x] = ob.n_y;
   }
   __syncthreads();
@@ -1365,18 +1469,17 @@ __global__ void k_expval_pauli_sv(const typename CplxT<R>::T* psi, int64_t dim, 
       if (o < o_cnt) {
         const uint64_t x = sx[o];
         const int64_t jx = j ^ static_cast<int64_t>(x);
-        // (P psi)_j = phase(j ^ x) psi_{j ^ x}
         const double sign = (__popcll(static_cast<uint64_t>(jx) & sz[o]) & 1) ? -sc[o] : sc[o];
         if (x == 0) {
-          acc[o] += sign * pa;
+          acc[o] = fma(sign, pa, acc[o]);
         } else {
           const double2 w = cmul(cconj(a), to_d2(p[jx]));
-          acc[o] += sign * re_iy(sy[o], w);
+          acc[o] = fma(sign, re_iy(sy[o], w), acc[o]);
         }
       }
     }
   }
-  block_reduce(acc, o_cnt, red);
+  block_reduce<kObsChunk>(acc, red);
   if (threadIdx.x < o_cnt) atomicAdd(&out[static_cast<int64_t>(inst) * n_obs + o_begin + threadIdx.x], acc[0]);
 }
 
@@ -1413,8 +1516,9 @@ __global__ void k_expval_dense_sv(const typename CplxT<R>::T* psi, int n, const 
       acc += va.x * row.x + va.y * row.y;
     }
   }
-  block_reduce(&acc, 1, red);
-  if (threadIdx.x == 0) atomicAdd(&out[static_cast<int64_t>(inst) * n_obs + oi], acc);
+  double accv[1] = {acc};
+  block_reduce<1>(accv, red);
+  if (threadIdx.x == 0) atomicAdd(&out[static_cast<int64_t>(inst) * n_obs + oi], accv[0]);
 }
 
 // Tr(coeff P rho) = coeff sum_k phase(k) rho[k][k ^ x]
@@ -1440,7 +1544,7 @@ __global__ void k_expval_pauli_dm(const typename CplxT<R>::T* rho, int64_t dim, 
       }
     }
   }
-  block_reduce(acc, o_cnt, red);
+  block_reduce<kObsChunk>(acc, red);
   if (threadIdx.x < o_cnt) atomicAdd(&out[static_cast<int64_t>(inst) * n_obs + o_begin + threadIdx.x], acc[0]);
 }
 
@@ -1475,8 +1579,9 @@ __global__ void k_expval_dense_dm(const typename CplxT<R>::T* rho, int n, const 
       }
     }
   }
-  block_reduce(&acc, 1, red);
-  if (threadIdx.x == 0) atomicAdd(&out[static_cast<int64_t>(inst) * n_obs + oi], acc);
+  double accv[1] = {acc};
+  block_reduce<1>(accv, red);
+  if (threadIdx.x == 0) atomicAdd(&out[static_cast<int64_t>(inst) * n_obs + oi], accv[0]);
 }
 
 // ---------------------------------------------------------------------------
@@ -1810,7 +1915,7 @@ int run_passes(const jq_plan* plan, const Schedule& sch, const TileOp* dops, con
     }
     const size_t smem = tile_smem<R>(pd, 1);
     const int64_t ntiles = (1LL << (plan->n_bits - pd.t)) * batch;
-    if (pd.step_end > pd.step_begin) {
+    if (pd.step_end > pd.step_begin && sch.reg_bits == RB) {
       const int threads = 1 << (pd.t - RB);
       const size_t elem = sizeof(typename CplxT<R>::T);
       const int nst = pd.step_end - pd.step_begin;
@@ -1876,12 +1981,17 @@ int measure(const jq_plan* plan, const DeviceTables* T, int batch, int out_type,
     int i = 0;
     while (i < n_obs) {
       if (plan->obs[i].kind == JQ_OBS_PAULI) {
+        // runs of Pauli words that are all Z strings (or all not), kObsChunk at most
+        const bool zdiag = plan->obs[i].x_mask == 0 && (plan->obs[i].z_mask >> 35) == 0;
         int j = i;
-        while (j < n_obs && j - i < kObsChunk && plan->obs[j].kind == JQ_OBS_PAULI) ++j;
+        while (j < n_obs && j - i < kObsChunk && plan->obs[j].kind == JQ_OBS_PAULI &&
+               (plan->obs[j].x_mask == 0 && (plan->obs[j].z_mask >> 35) == 0) == zdiag)
+          ++j;
         const int gx = std::max(1, std::min<int>(static_cast<int>((dim + threads - 1) / threads),
                                                  std::max(1, 4 * sm_count() / std::max(batch, 1))));
         dim3 grid(gx, batch);
         if (dm) k_expval_pauli_dm<R><<<grid, threads, 0, st>>>(state, dim, od, i, j - i, o, n_obs);
+        else if (zdiag) k_expval_zdiag_sv<R><<<grid, threads, 0, st>>>(state, dim, od, i, j - i, o, n_obs);
         else k_expval_pauli_sv<R><<<grid, threads, 0, st>>>(state, dim, od, i, j - i, o, n_obs);
         i = j;
       } else {

@@ -237,7 +237,10 @@ uint32_t swz_bit(int pos, int dtype) {
 // deferred op, is deferred to a later stage.  Ops with more targets than the
 // register forms cover run as generic shared-memory steps.
 void build_steps(Schedule& s, const std::vector<int32_t>& perm_pool, int dtype) {
-  const int r = 4;
+  // register bits per stage (amplitudes per thread = 2^r); JQ_REG_BITS=3
+  // selects 8 amplitudes per thread (more threads, more stages)
+  int r = 4;
+  if (const char* e = std::getenv("JQ_REG_BITS")) r = (std::atoi(e) == 3) ? 3 : 4;
   s.reg_bits = r;
   for (PassDesc& pd : s.passes) {
     pd.step_begin = pd.step_end = static_cast<int32_t>(s.steps.size());
@@ -298,16 +301,35 @@ void build_steps(Schedule& s, const std::vector<int32_t>& perm_pool, int dtype) 
       for (int pos = t - 1; pos >= 0 && __builtin_popcount(R) < r; --pos) R |= 1u << pos;
       int rank_r[32], rank_t[32];
       int nr = 0, nt = 0;
+      // Thread-bit order: the lowest lane bits (the lanes of one shared-memory
+      // wavefront: 16 for 8-byte, 8 for 16-byte amplitudes) take positions of
+      // distinct swizzle classes pos % nbank, so a stage access hits distinct
+      // bank groups; the other thread bits follow in ascending order.
+      const int nbank = (dtype == JQ_C64) ? 4 : 3;
+      std::vector<int> tpos, first, rest;
+      for (int pos = 0; pos < t; ++pos)
+        if (!(R >> pos & 1u)) tpos.push_back(pos);
+      uint32_t classes = 0;
+      for (int pos : tpos) {
+        const uint32_t cb = 1u << (pos % nbank);
+        if (static_cast<int>(first.size()) < nbank && !(classes & cb)) {
+          classes |= cb;
+          first.push_back(pos);
+        } else {
+          rest.push_back(pos);
+        }
+      }
+      first.insert(first.end(), rest.begin(), rest.end());
       for (int pos = 0; pos < t; ++pos) {
+        rank_r[pos] = rank_t[pos] = -1;
         if (R >> pos & 1u) {
           st.ebits[nr] = swz_bit(pos, dtype);
           rank_r[pos] = nr++;
-          rank_t[pos] = -1;
-        } else {
-          st.tbits[nt] = swz_bit(pos, dtype);
-          rank_t[pos] = nt++;
-          rank_r[pos] = -1;
         }
+      }
+      for (int pos : first) {
+        st.tbits[nt] = swz_bit(pos, dtype);
+        rank_t[pos] = nt++;
       }
       st.kind = 0;
       st.a = static_cast<int32_t>(s.rops.size());
