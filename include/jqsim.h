@@ -261,6 +261,50 @@ JQ_API int jq_backward(const jq_plan* plan, int batch, const double* angles,
                 double* grad_angles, void* grad_mats, void* grad_init,
                 void* workspace, size_t workspace_bytes, void* stream);
 
+/* ------------------------------------------------------------------------
+ * Batched uneven instances: forward + adjoint of many independent circuits
+ * of different qubit counts, depths and parameters in one CUDA-graph launch.
+ * Replaces the reference's batched trace of _single_execute under vmap /
+ * shard_map (jaqsi/script.py:426-434, :87-125) for gradient workloads.
+ *
+ * Instance i runs plans[plan_of[i]]; every plan is a unitary statevector
+ * plan of one dtype with Pauli or dense observables and no matrix
+ * arguments.  Angles and gradients are concatenated per instance in order
+ * (instance i owns n_angles(plan) entries), expectation values likewise
+ * (n_obs(plan) entries).
+ * ---------------------------------------------------------------------- */
+typedef struct jq_batch jq_batch;
+
+typedef struct jq_batch_config {
+  int32_t warp_max_qubits; /* n <= this: one warp per instance, state in shared memory */
+  int32_t cta_max_qubits;  /* n <= this: one CTA per instance, state in shared memory  */
+  int32_t warp_threads;    /* threads per CTA of the warp-per-instance kernel (32..512) */
+  int32_t cta_threads;     /* threads per CTA of the CTA-per-instance kernel (64..512)  */
+} jq_batch_config;
+
+/* cfg NULL: defaults (complex64 9 / 13 qubits, complex128 8 / 12; 256 / 512 threads). */
+JQ_API int jq_batch_build(jq_plan* const* plans, int n_plans, const int32_t* plan_of, int n_inst,
+                          const jq_batch_config* cfg, jq_batch** out);
+JQ_API int jq_batch_free(jq_batch* batch);
+/* totals: angles (= gradient entries) and expectation values over all
+ * instances; n_class[3] = instances in the warp, cta and tile classes. */
+JQ_API int jq_batch_info(const jq_batch* batch, int64_t* n_angles, int64_t* n_obs, int32_t* n_class,
+                         jq_batch_config* cfg);
+/* Workspace for jq_batch_run under the current configuration and under
+ * every configuration jq_batch_autotune tries (the maximum). */
+JQ_API size_t jq_batch_workspace_bytes(const jq_batch* batch);
+JQ_API int jq_batch_set_config(jq_batch* batch, const jq_batch_config* cfg);
+/* Expectation values and d(sum_o ct_o <O_o>)/d angles of every instance
+ * (ct: float64 [n_obs total] or NULL for all ones); device pointers.  The
+ * first call with a set of pointers captures a CUDA graph, later calls with
+ * the same pointers replay it. */
+JQ_API int jq_batch_run(jq_batch* batch, const double* angles, const double* ct, double* expval, double* grad,
+                        void* workspace, size_t workspace_bytes, void* stream);
+/* Time candidate configurations on these inputs, keep the fastest (also
+ * returned in *chosen when non-NULL).  Synchronises the stream. */
+JQ_API int jq_batch_autotune(jq_batch* batch, const double* angles, double* expval, double* grad,
+                             void* workspace, size_t workspace_bytes, void* stream, jq_batch_config* chosen);
+
 /* Message of the last failed call on this thread ("" if none). */
 JQ_API const char* jq_last_error(void);
 

@@ -19,12 +19,13 @@ from jaqsi_b200.noise import (
 from jaqsi_b200.script import Script, make_hashable
 from jaqsi_b200.tape import copy_to_tape, recording, shift_and_append
 from jaqsi_b200 import simulation
+from jaqsi_b200.batch import BatchedGradients
 
 __version__ = "0.1.0"
 
 __all__ = [
     "Script", "Operation", "Hermitian", "GateStructure", "cdtype", "set_default_dtype", "make_hashable",
-    "recording", "copy_to_tape", "shift_and_append", "simulation", "build_parity_observable",
+    "recording", "copy_to_tape", "shift_and_append", "simulation", "build_parity_observable", "BatchedGradients",
     "Id", "PauliX", "PauliY", "PauliZ", "H", "S", "SWAP", "RX", "RY", "RZ", "Rot", "CX", "CY", "CZ", "CCX",
     "CSWAP", "CRX", "CRY", "CRZ", "ControlledPhaseShift", "PauliRot", "RXX", "RYY", "RZZ", "RZX",
     "ControlledPauliRot", "DiagonalQubitUnitary", "RandomUnitary", "Barrier",

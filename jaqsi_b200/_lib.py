@@ -51,6 +51,13 @@ EXPORTED = (
     "jq_sweep",
     "jq_adjoint",
     "jq_backward",
+    "jq_batch_build",
+    "jq_batch_free",
+    "jq_batch_info",
+    "jq_batch_workspace_bytes",
+    "jq_batch_set_config",
+    "jq_batch_run",
+    "jq_batch_autotune",
     "jq_last_error",
     "jq_version",
 )
@@ -127,6 +134,18 @@ class JqPlanInfo(ctypes.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
+class JqBatchConfig(ctypes.Structure):
+    _fields_ = [
+        ("warp_max_qubits", ctypes.c_int32),
+        ("cta_max_qubits", ctypes.c_int32),
+        ("warp_threads", ctypes.c_int32),
+        ("cta_threads", ctypes.c_int32),
+    ]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
 _LIB: Optional[ctypes.CDLL] = None
 _LOCK = threading.Lock()
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libjqsim.so")
@@ -160,6 +179,22 @@ def _declare(lib: ctypes.CDLL) -> None:
     lib.jq_adjoint.restype = i32
     lib.jq_backward.argtypes = [vp, i32, vp, vp, vp, i32, i32, vp, vp, vp, vp, vp, vp, ctypes.c_size_t, vp]
     lib.jq_backward.restype = i32
+    lib.jq_batch_build.argtypes = [ctypes.POINTER(vp), i32, ctypes.POINTER(ctypes.c_int32), i32,
+                                   ctypes.POINTER(JqBatchConfig), ctypes.POINTER(vp)]
+    lib.jq_batch_build.restype = i32
+    lib.jq_batch_free.argtypes = [vp]
+    lib.jq_batch_free.restype = i32
+    lib.jq_batch_info.argtypes = [vp, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64),
+                                  ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(JqBatchConfig)]
+    lib.jq_batch_info.restype = i32
+    lib.jq_batch_workspace_bytes.argtypes = [vp]
+    lib.jq_batch_workspace_bytes.restype = ctypes.c_size_t
+    lib.jq_batch_set_config.argtypes = [vp, ctypes.POINTER(JqBatchConfig)]
+    lib.jq_batch_set_config.restype = i32
+    lib.jq_batch_run.argtypes = [vp, vp, vp, vp, vp, vp, ctypes.c_size_t, vp]
+    lib.jq_batch_run.restype = i32
+    lib.jq_batch_autotune.argtypes = [vp, vp, vp, vp, vp, ctypes.c_size_t, vp, ctypes.POINTER(JqBatchConfig)]
+    lib.jq_batch_autotune.restype = i32
     lib.jq_last_error.argtypes = []
     lib.jq_last_error.restype = ctypes.c_char_p
     lib.jq_version.argtypes = []

@@ -12,7 +12,9 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
+#include <memory>
 #include <mutex>
 #include <string>
 
@@ -1114,25 +1116,19 @@ __global__ void __launch_bounds__(512, 1) k_tile_bwd(const typename CplxT<R>::T*
 // ---------------------------------------------------------------------------
 // block matrices: fuse each block's prims in float64, round to the run dtype
 // ---------------------------------------------------------------------------
+// Inner matrix (or diagonal) of one block of one instance into bm (the
+// instance's block matrices); `sc` is the instance's scratch (k > 2 blocks).
 template <typename R>
-__global__ void k_prep(const DevBlock* __restrict__ blocks, int nblocks, const DevPrim* __restrict__ prims,
-                       const DevOp* __restrict__ ops, const double* __restrict__ angles, int n_angles,
-                       const double2* __restrict__ mats, int n_mats, const double2* __restrict__ cpool,
-                       typename CplxT<R>::T* __restrict__ bmat, int64_t bmat_stride, double2* scratch,
-                       int64_t scratch_stride, int batch) {
+__device__ void prep_block(const DevBlock& blk, const DevPrim* __restrict__ prims, const DevOp* __restrict__ ops,
+                           const double* ang, const double2* mt, const double2* __restrict__ cpool,
+                           typename CplxT<R>::T* bm, double2* sc) {
   using C = typename CplxT<R>::T;
-  const int64_t idx = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (idx >= static_cast<int64_t>(batch) * nblocks) return;
-  const int inst = static_cast<int>(idx / nblocks), b = static_cast<int>(idx % nblocks);
-  const DevBlock blk = blocks[b];
   if (blk.kind == BK_PERM) return;
-  const double* ang = angles ? angles + static_cast<int64_t>(inst) * n_angles : nullptr;
-  const double2* mt = mats ? mats + static_cast<int64_t>(inst) * n_mats : nullptr;
   const int d = 1 << blk.k;
   double2 la[16], lb[16], lc[16];
   double2 *acc = la, *pm = lb, *tmp = lc;
   if (blk.k > 2) {
-    double2* sc = scratch + inst * scratch_stride + blk.scratch_off;
+    sc += blk.scratch_off;
     acc = sc;
     pm = sc + d * d;
     tmp = sc + 2 * d * d;
@@ -1143,7 +1139,7 @@ __global__ void k_prep(const DevBlock* __restrict__ blocks, int nblocks, const D
     m_mul(pm, acc, tmp, d);
     m_copy(tmp, acc, d);
   }
-  C* out = bmat + inst * bmat_stride + blk.mat_off;
+  C* out = bm + blk.mat_off;
   const int base = d - blk.d;
   if (blk.kind == BK_DIAG) {
     for (int i = 0; i < blk.d; ++i) {
@@ -1159,27 +1155,37 @@ __global__ void k_prep(const DevBlock* __restrict__ blocks, int nblocks, const D
   }
 }
 
-// ---------------------------------------------------------------------------
-// chain rule: block cotangents -> per-prim cotangents -> angles / matrices
-// ---------------------------------------------------------------------------
-__global__ void k_chain(const DevBlock* __restrict__ blocks, int nblocks, const DevPrim* __restrict__ prims,
-                        const DevOp* __restrict__ ops, const double* __restrict__ angles, int n_angles,
-                        const double2* __restrict__ mats, int n_mats, const double2* __restrict__ cpool,
-                        const double2* __restrict__ gacc, int64_t grad_stride, double2* scratch,
-                        int64_t scratch_stride, int batch, double* grad_angles, double2* grad_mats) {
+template <typename R>
+__global__ void k_prep(const DevBlock* __restrict__ blocks, int nblocks, const DevPrim* __restrict__ prims,
+                       const DevOp* __restrict__ ops, const double* __restrict__ angles, int n_angles,
+                       const double2* __restrict__ mats, int n_mats, const double2* __restrict__ cpool,
+                       typename CplxT<R>::T* __restrict__ bmat, int64_t bmat_stride, double2* scratch,
+                       int64_t scratch_stride, int batch) {
   const int64_t idx = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (idx >= static_cast<int64_t>(batch) * nblocks) return;
   const int inst = static_cast<int>(idx / nblocks), b = static_cast<int>(idx % nblocks);
   const DevBlock blk = blocks[b];
-  if (blk.grad_off < 0) return;
   const double* ang = angles ? angles + static_cast<int64_t>(inst) * n_angles : nullptr;
   const double2* mt = mats ? mats + static_cast<int64_t>(inst) * n_mats : nullptr;
-  const double2* ga = gacc + inst * grad_stride + blk.grad_off;
+  prep_block<R>(blk, prims, ops, ang, mt, cpool, bmat + inst * bmat_stride, scratch + inst * scratch_stride);
+}
+
+// ---------------------------------------------------------------------------
+// chain rule: block cotangents -> per-prim cotangents -> angles / matrices
+// ---------------------------------------------------------------------------
+// Chain rule of one block of one instance: block cotangent (gacc: the
+// instance's accumulators) -> per-prim cotangents -> angle / matrix gradients
+// (ga_out / gm_out: the instance's gradient rows, accumulated atomically).
+__device__ void chain_block(const DevBlock& blk, const DevPrim* __restrict__ prims, const DevOp* __restrict__ ops,
+                            const double* ang, const double2* mt, const double2* __restrict__ cpool,
+                            const double2* gacc, double2* sc, double* ga_out, double2* gm_out) {
+  if (blk.grad_off < 0) return;
+  const double2* ga = gacc + blk.grad_off;
   const int d = 1 << blk.k;
   double2 l0[16], l1[16], l2[16], l3[16], l4[16], l5[16];
   double2 *Gb = l0, *A = l1, *B = l2, *P = l3, *T = l4, *T2 = l5;
   if (blk.k > 2) {
-    double2* sc = scratch + inst * scratch_stride + blk.scratch_off;
+    sc += blk.scratch_off;
     Gb = sc; A = sc + d * d; B = sc + 2 * d * d; P = sc + 3 * d * d; T = sc + 4 * d * d; T2 = sc + 5 * d * d;
   }
   m_zero(Gb, d);
@@ -1215,8 +1221,8 @@ __global__ void k_chain(const DevBlock* __restrict__ blocks, int nblocks, const 
     m_mul_ah(A, Gb, T, d);
     m_mul_bh(T, B, A, d);  // A now holds grad_P
     if (op.kind == JQ_K_MATRIX) {
-      if (!grad_mats) continue;
-      double2* gm = grad_mats + static_cast<int64_t>(inst) * n_mats + op.mat_slot;
+      if (!gm_out) continue;
+      double2* gm = gm_out + op.mat_slot;
       const int du = 1 << op.k;
       if (p.form == PF_U || p.form == PF_CONJ) {
         const double sgn = (p.form == PF_CONJ) ? -1.0 : 1.0;
@@ -1255,13 +1261,29 @@ __global__ void k_chain(const DevBlock* __restrict__ blocks, int nblocks, const 
       }
       continue;
     }
-    if (!grad_angles) continue;
+    if (!ga_out) continue;
     for (int j = 0; j < op.n_angles; ++j) {
       prim_matrix(p, ops, ang, mt, cpool, P, j, T2);
       const double g = m_inner_re(A, P, d);
-      atomicAdd(&grad_angles[static_cast<int64_t>(inst) * n_angles + op.angle_slot + j], g);
+      atomicAdd(&ga_out[op.angle_slot + j], g);
     }
   }
+}
+
+__global__ void k_chain(const DevBlock* __restrict__ blocks, int nblocks, const DevPrim* __restrict__ prims,
+                        const DevOp* __restrict__ ops, const double* __restrict__ angles, int n_angles,
+                        const double2* __restrict__ mats, int n_mats, const double2* __restrict__ cpool,
+                        const double2* __restrict__ gacc, int64_t grad_stride, double2* scratch,
+                        int64_t scratch_stride, int batch, double* grad_angles, double2* grad_mats) {
+  const int64_t idx = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (idx >= static_cast<int64_t>(batch) * nblocks) return;
+  const int inst = static_cast<int>(idx / nblocks), b = static_cast<int>(idx % nblocks);
+  const DevBlock blk = blocks[b];
+  const double* ang = angles ? angles + static_cast<int64_t>(inst) * n_angles : nullptr;
+  const double2* mt = mats ? mats + static_cast<int64_t>(inst) * n_mats : nullptr;
+  chain_block(blk, prims, ops, ang, mt, cpool, gacc + inst * grad_stride, scratch + inst * scratch_stride,
+              grad_angles ? grad_angles + static_cast<int64_t>(inst) * n_angles : nullptr,
+              grad_mats ? grad_mats + static_cast<int64_t>(inst) * n_mats : nullptr);
 }
 
 // ---------------------------------------------------------------------------
@@ -2288,6 +2310,87 @@ int backward_impl(const jq_plan* plan, int batch, const double* angles, const vo
   return JQ_OK;
 }
 
+#include "batch.cuh"
+
+jq_batch_config batch_default_config(int dtype) {
+  jq_batch_config c;
+  c.warp_max_qubits = dtype == JQ_C64 ? 9 : 8;
+  c.cta_max_qubits = dtype == JQ_C64 ? 13 : 12;
+  c.warp_threads = 256;
+  c.cta_threads = 512;
+  return c;
+}
+
+bool batch_config_ok(const jq_batch_config& c) {
+  return c.warp_max_qubits >= 0 && c.warp_max_qubits <= 12 && c.cta_max_qubits >= 0 && c.cta_max_qubits <= 14 &&
+         c.warp_threads >= 32 && c.warp_threads <= 512 && (c.warp_threads % 32) == 0 && c.cta_threads >= 64 &&
+         c.cta_threads <= 512 && (c.cta_threads % 32) == 0;
+}
+
+std::vector<jq_batch_config> batch_candidates(const jq_batch* b) {
+  std::vector<jq_batch_config> out;
+  const bool c64 = b->dtype == JQ_C64;
+  const int wmax[] = {5, 7, 8, 9, 10};
+  const int cmax_c64[] = {12, 13};
+  const int cmax_c128[] = {11, 12};
+  for (int wm : wmax) {
+    if (!c64 && wm > 9) continue;
+    for (int cm : (c64 ? cmax_c64 : cmax_c128))
+      for (int wt : {128, 256})
+        for (int ct : {256, 512}) {
+          jq_batch_config c{wm, cm, wt, ct};
+          const int elem = c64 ? 8 : 16;
+          if (batch_smem(wm, wt / 32, elem) > 227 * 1024) continue;
+          out.push_back(c);
+        }
+  }
+  return out;
+}
+
+template <typename R>
+int batch_run_graph(jq_batch* b, const double* angles, const double* ct, double* expval, double* grad, void* ws,
+                    cudaStream_t st) {
+  if (std::getenv("JQ_BATCH_NO_GRAPH")) {
+    // the same launches without the CUDA graph (debugging, timing breakdowns)
+    if (int rc = set_smem_attrs<R>()) return rc;
+    return batch_enqueue<R>(b, angles, ct, expval, grad, static_cast<char*>(ws), st);
+  }
+  const void* key[7] = {angles, ct, expval, grad, ws, st, nullptr};
+  bool same = b->graph != nullptr;
+  for (int i = 0; i < 6 && same; ++i) same = key[i] == b->graph_key[i];
+  if (!same) {
+    if (b->graph) {
+      cudaGraphExecDestroy(b->graph);
+      b->graph = nullptr;
+    }
+    // everything that allocates or uploads happens before the capture
+    if (int rc = set_smem_attrs<R>()) return rc;
+    for (const auto& tg : b->tiles) {
+      const DeviceTables* T = nullptr;
+      if (int rc = device_tables(b->plans[tg.plan], &T)) return rc;
+    }
+    JQ_CUDA(cudaStreamBeginCapture(b->cap, cudaStreamCaptureModeThreadLocal));
+    const int rc = batch_enqueue<R>(b, angles, ct, expval, grad, static_cast<char*>(ws), b->cap);
+    cudaGraph_t g = nullptr;
+    const cudaError_t ce = cudaStreamEndCapture(b->cap, &g);
+    if (rc || ce != cudaSuccess) {
+      if (g) cudaGraphDestroy(g);
+      if (!rc) set_error(std::string("graph capture of the batch failed: ") + cudaGetErrorString(ce));
+      return rc ? rc : JQ_ECUDA;
+    }
+    const cudaError_t ie = cudaGraphInstantiate(&b->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (ie != cudaSuccess) {
+      b->graph = nullptr;
+      set_error(std::string("graph instantiation of the batch failed: ") + cudaGetErrorString(ie));
+      return JQ_ECUDA;
+    }
+    for (int i = 0; i < 6; ++i) b->graph_key[i] = key[i];
+  }
+  JQ_CUDA(cudaGraphLaunch(b->graph, st));
+  return JQ_OK;
+}
+
 }  // namespace
 }  // namespace jq
 
@@ -2512,6 +2615,248 @@ int jq_forward_noalloc(const jq_plan* plan, int batch, const double* angles, con
   }
   return jq_forward(plan, batch, angles, mats, init, init_batched, out_type, state, out, ws, JQ_STATIC_WS_BYTES,
                     stream);
+}
+
+// ---------------------------------------------------------------------------
+// batched uneven instances
+// ---------------------------------------------------------------------------
+int jq_batch_build(jq_plan* const* plans, int n_plans, const int32_t* plan_of, int n_inst,
+                   const jq_batch_config* cfg, jq_batch** out) {
+  if (!out || !plans || n_plans <= 0 || n_inst <= 0 || !plan_of) {
+    set_error("jq_batch_build: need plans, plan_of and n_inst > 0");
+    return JQ_EINVAL;
+  }
+  *out = nullptr;
+  std::unique_ptr<jq_batch> b(new jq_batch());
+  b->dtype = plans[0]->dtype;
+  cudaGetDevice(&b->device);
+  b->sm_count = sm_count();
+  for (int p = 0; p < n_plans; ++p) {
+    const jq_plan* pl = plans[p];
+    if (!pl || pl->mode != JQ_STATEVECTOR || !pl->unitary || pl->n_mats > 0 || pl->dtype != b->dtype) {
+      set_error("jq_batch_build: plan " + std::to_string(p) +
+                " is not a unitary statevector plan without matrix arguments of the batch dtype");
+      return JQ_EINVAL;
+    }
+    b->plans.push_back(pl);
+    b->n_of_plan.push_back(pl->n_qubits);
+    BPlan bp;
+    std::memset(&bp, 0, sizeof(bp));
+    bp.n = pl->n_qubits;
+    bp.nblocks = static_cast<int32_t>(pl->blocks.size());
+    bp.blk_off = static_cast<int32_t>(b->dblk.size());
+    bp.n_angles = pl->n_angles;
+    bp.obs_off = static_cast<int32_t>(b->obs.size());
+    bp.n_obs = static_cast<int32_t>(pl->obs.size());
+    bp.bmat_stride = static_cast<int32_t>(pl->bmat_stride);
+    bp.grad_stride = static_cast<int32_t>(pl->grad_stride);
+    const int32_t prim_base = static_cast<int32_t>(b->prims.size());
+    const int32_t op_base = static_cast<int32_t>(b->ops.size());
+    const int32_t cpool_base = static_cast<int32_t>(b->cpool.size() / 2);
+    for (size_t i = 0; i < pl->blocks.size(); ++i) {
+      DevBlock blk = pl->blocks[i];
+      BBlock bb;
+      std::memset(&bb, 0, sizeof(bb));
+      bb.kind = blk.kind;
+      bb.nt = blk.k - blk.n_ctrl;
+      bb.grad_off = blk.grad_off;
+      bb.mat_off = blk.mat_off;
+      const auto& wires = pl->block_wires[i];
+      for (int c = 0; c < blk.n_ctrl; ++c) bb.cmask |= 1u << (pl->n_bits - 1 - wires[c]);
+      bb.tb0 = bb.nt >= 1 ? pl->n_bits - 1 - wires[blk.n_ctrl] : 0;
+      bb.tb1 = bb.nt >= 2 ? pl->n_bits - 1 - wires[blk.n_ctrl + 1] : 0;
+      if (blk.kind == BK_PERM && bb.nt >= 1 && bb.nt <= 2)
+        for (int r = 0; r < (1 << bb.nt); ++r) bb.perm |= (pl->perm_pool[blk.perm_off + r] & 3) << (2 * r);
+      b->bblk.push_back(bb);
+      blk.prim_begin += prim_base;
+      blk.prim_end += prim_base;
+      b->dblk.push_back(blk);
+    }
+    for (DevPrim pr : pl->prims) {
+      if (pr.op >= 0) pr.op += op_base;
+      if (pr.form == PF_CONST) pr.const_off += cpool_base;
+      b->prims.push_back(pr);
+    }
+    for (const DevOp& o : pl->ops) b->ops.push_back(o);
+    b->cpool.insert(b->cpool.end(), pl->const_pool.begin(), pl->const_pool.end());
+    for (const DevObs& o : pl->obs) b->obs.push_back(o);
+    b->bplans.push_back(bp);
+  }
+  int64_t ang = 0, outs = 0;
+  for (int i = 0; i < n_inst; ++i) {
+    const int p = plan_of[i];
+    if (p < 0 || p >= n_plans) {
+      set_error("jq_batch_build: plan_of[" + std::to_string(i) + "] out of range");
+      return JQ_EINVAL;
+    }
+    BInst bi;
+    std::memset(&bi, 0, sizeof(bi));
+    bi.plan = p;
+    bi.angle_off = ang;
+    bi.out_off = outs;
+    ang += b->plans[p]->n_angles;
+    outs += static_cast<int64_t>(b->plans[p]->obs.size());
+    b->inst.push_back(bi);
+  }
+  b->n_inst = n_inst;
+  b->n_angles_total = ang;
+  b->n_obs_total = outs;
+  b->cfg = cfg ? *cfg : batch_default_config(b->dtype);
+  if (!batch_config_ok(b->cfg)) {
+    set_error("jq_batch_build: configuration out of range");
+    return JQ_EINVAL;
+  }
+  auto up = [](const void* src, size_t bytes, void** dst) -> int {
+    if (bytes == 0) bytes = 16;
+    if (cudaMalloc(dst, bytes) != cudaSuccess) return JQ_ECUDA;
+    if (src && cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice) != cudaSuccess) return JQ_ECUDA;
+    return JQ_OK;
+  };
+  if (b->cpool.empty()) b->cpool.assign(2, 0.0);
+  if (up(b->bplans.data(), b->bplans.size() * sizeof(BPlan), &b->d_plans) ||
+      up(b->inst.data(), b->inst.size() * sizeof(BInst), &b->d_inst) ||
+      up(b->bblk.data(), b->bblk.size() * sizeof(BBlock), &b->d_bblk) ||
+      up(b->dblk.data(), b->dblk.size() * sizeof(DevBlock), &b->d_dblk) ||
+      up(b->prims.data(), b->prims.size() * sizeof(DevPrim), &b->d_prims) ||
+      up(b->ops.data(), b->ops.size() * sizeof(DevOp), &b->d_ops) ||
+      up(b->cpool.data(), b->cpool.size() * sizeof(double), &b->d_cpool) ||
+      up(b->obs.data(), b->obs.size() * sizeof(DevObs), &b->d_obs)) {
+    set_error("jq_batch_build: upload of the batch tables failed");
+    return JQ_ECUDA;
+  }
+  for (int i = 0; i < 2; ++i)
+    if (cudaStreamCreateWithFlags(&b->side[i], cudaStreamNonBlocking) != cudaSuccess) return JQ_ECUDA;
+  if (cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking) != cudaSuccess) return JQ_ECUDA;
+  for (int i = 0; i < 4; ++i)
+    if (cudaEventCreateWithFlags(&b->ev[i], cudaEventDisableTiming) != cudaSuccess) return JQ_ECUDA;
+  if (int rc = batch_classify(b.get())) return rc;
+  *out = b.release();
+  return JQ_OK;
+}
+
+int jq_batch_free(jq_batch* b) {
+  if (!b) return JQ_OK;
+  if (b->graph) cudaGraphExecDestroy(b->graph);
+  void* bufs[] = {b->d_plans, b->d_inst, b->d_bblk, b->d_dblk, b->d_prims, b->d_ops, b->d_cpool, b->d_obs,
+                  b->d_order, b->d_tile_off};
+  for (void* p : bufs)
+    if (p) cudaFree(p);
+  for (int i = 0; i < 2; ++i)
+    if (b->side[i]) cudaStreamDestroy(b->side[i]);
+  if (b->cap) cudaStreamDestroy(b->cap);
+  for (int i = 0; i < 4; ++i)
+    if (b->ev[i]) cudaEventDestroy(b->ev[i]);
+  delete b;
+  return JQ_OK;
+}
+
+int jq_batch_info(const jq_batch* b, int64_t* n_angles, int64_t* n_obs, int32_t* n_class, jq_batch_config* cfg) {
+  if (!b) {
+    set_error("jq_batch_info: NULL batch");
+    return JQ_EINVAL;
+  }
+  if (n_angles) *n_angles = b->n_angles_total;
+  if (n_obs) *n_obs = b->n_obs_total;
+  if (n_class) {
+    n_class[0] = static_cast<int32_t>(b->order_warp.size());
+    n_class[1] = static_cast<int32_t>(b->order_cta.size());
+    int32_t t = 0;
+    for (const auto& tg : b->tiles) t += static_cast<int32_t>(tg.members.size());
+    n_class[2] = t;
+  }
+  if (cfg) *cfg = b->cfg;
+  return JQ_OK;
+}
+
+size_t jq_batch_workspace_bytes(const jq_batch* cb) {
+  if (!cb) return 0;
+  jq_batch* b = const_cast<jq_batch*>(cb);
+  size_t need = batch_ws_for(b, b->cfg);
+  for (const jq_batch_config& c : batch_candidates(b)) need = std::max(need, batch_ws_for(b, c));
+  return need;
+}
+
+int jq_batch_set_config(jq_batch* b, const jq_batch_config* cfg) {
+  if (!b || !cfg || !batch_config_ok(*cfg)) {
+    set_error("jq_batch_set_config: configuration out of range");
+    return JQ_EINVAL;
+  }
+  const jq_batch_config keep = b->cfg;
+  b->cfg = *cfg;
+  if (int rc = batch_classify(b)) {
+    b->cfg = keep;
+    batch_classify(b);
+    return rc;
+  }
+  return JQ_OK;
+}
+
+int jq_batch_run(jq_batch* b, const double* angles, const double* ct, double* expval, double* grad, void* ws,
+                 size_t ws_bytes, void* stream) {
+  if (!b || (!angles && b->n_angles_total > 0) || !expval || (!grad && b->n_angles_total > 0)) {
+    set_error("jq_batch_run: need a batch, angles, expval and grad buffers");
+    return JQ_EINVAL;
+  }
+  if (ws_bytes < b->ws_total || !ws) {
+    set_error("workspace too small: need " + std::to_string(b->ws_total) + " bytes");
+    return JQ_ENOMEM;
+  }
+  int dev = -1;
+  cudaGetDevice(&dev);
+  if (dev != b->device) {
+    set_error("jq_batch_run: the batch was built on device " + std::to_string(b->device));
+    return JQ_EINVAL;
+  }
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (b->dtype == JQ_C64) return batch_run_graph<float>(b, angles, ct, expval, grad, ws, st);
+  return batch_run_graph<double>(b, angles, ct, expval, grad, ws, st);
+}
+
+int jq_batch_autotune(jq_batch* b, const double* angles, double* expval, double* grad, void* ws, size_t ws_bytes,
+                      void* stream, jq_batch_config* chosen) {
+  if (!b) {
+    set_error("jq_batch_autotune: NULL batch");
+    return JQ_EINVAL;
+  }
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  cudaEvent_t e0, e1;
+  JQ_CUDA(cudaEventCreate(&e0));
+  JQ_CUDA(cudaEventCreate(&e1));
+  const jq_batch_config start = b->cfg;
+  jq_batch_config best = start;
+  float best_ms = -1.0f;
+  std::vector<jq_batch_config> cands = batch_candidates(b);
+  cands.insert(cands.begin(), start);
+  int rc = JQ_OK;
+  for (const jq_batch_config& c : cands) {
+    if (batch_ws_for(b, c) > ws_bytes) continue;
+    if ((rc = jq_batch_set_config(b, &c))) continue;
+    // one warm-up run (captures the graph), then one timed replay
+    if ((rc = jq_batch_run(b, angles, nullptr, expval, grad, ws, ws_bytes, stream))) continue;
+    cudaEventRecord(e0, st);
+    if ((rc = jq_batch_run(b, angles, nullptr, expval, grad, ws, ws_bytes, stream))) continue;
+    cudaEventRecord(e1, st);
+    if (cudaEventSynchronize(e1) != cudaSuccess) {
+      rc = JQ_ECUDA;
+      break;
+    }
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (best_ms < 0.0f || ms < best_ms) {
+      best_ms = ms;
+      best = c;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (best_ms < 0.0f) {
+    if (!rc) set_error("jq_batch_autotune: no candidate fits the workspace");
+    jq_batch_set_config(b, &start);
+    return rc ? rc : JQ_ENOMEM;
+  }
+  if ((rc = jq_batch_set_config(b, &best))) return rc;
+  if (chosen) *chosen = best;
+  return JQ_OK;
 }
 
 const char* jq_last_error(void) { return g_last_error.c_str(); }

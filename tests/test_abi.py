@@ -41,14 +41,15 @@ def test_struct_layouts_match_header(tmp_path):
     src = tmp_path / "sz.c"
     src.write_text(
         '#include <stdio.h>\n#include <stddef.h>\n#include "jqsim.h"\n'
-        "int main(void){printf(\"%zu %zu %zu %zu %zu %zu\\n\", sizeof(jq_op), sizeof(jq_obs), sizeof(jq_tune),"
-        " sizeof(jq_plan_info), offsetof(jq_op, const_mat), offsetof(jq_obs, mat));return 0;}\n"
+        "int main(void){printf(\"%zu %zu %zu %zu %zu %zu %zu\\n\", sizeof(jq_op), sizeof(jq_obs), sizeof(jq_tune),"
+        " sizeof(jq_plan_info), offsetof(jq_op, const_mat), offsetof(jq_obs, mat), sizeof(jq_batch_config));"
+        "return 0;}\n"
     )
     exe = tmp_path / "sz"
     subprocess.run(["gcc", "-I", os.path.dirname(HEADER), str(src), "-o", str(exe)], check=True)
     got = [int(v) for v in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
     want = [ctypes.sizeof(L.JqOp), ctypes.sizeof(L.JqObs), ctypes.sizeof(L.JqTune), ctypes.sizeof(L.JqPlanInfo),
-            L.JqOp.const_mat.offset, L.JqObs.mat.offset]
+            L.JqOp.const_mat.offset, L.JqObs.mat.offset, ctypes.sizeof(L.JqBatchConfig)]
     assert got == want
 
 

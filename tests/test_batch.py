@@ -1,0 +1,101 @@
+"""Batched uneven instances (jq_batch): expectation values and full adjoint
+gradients of many independent circuits in one CUDA-graph launch, against the
+oracle's per-instance adjoint gradient.  Instances span all three classes
+(one per warp, one per CTA, batched tile passes) by choosing the class
+thresholds explicitly.
+"""
+import numpy as np
+import pytest
+import torch
+
+import jaqsi_b200 as jq
+from oracle import sim_np as O
+from tests.helpers import obs_records, random_circuit, to_records
+
+pytestmark = pytest.mark.gpu
+
+TOL = {torch.complex64: 1e-5, torch.complex128: 1e-10}
+
+
+def _instances(seed, count, nmin, nmax, with_dense=True):
+    rng = np.random.default_rng(seed)
+    inst, refs = [], []
+    for i in range(count):
+        n = int(rng.integers(nmin, nmax + 1))
+        depth = int(rng.integers(3, 14))
+        params = torch.tensor(rng.uniform(0, 2 * np.pi, 20 * depth + 10))
+        with jq.recording() as tape:
+            random_circuit(n, depth, np.random.default_rng(1000 + i), params, wide=False)
+        obs = [jq.PauliZ(wires=int(rng.integers(n))), jq.PauliX(wires=int(rng.integers(n)))]
+        if n >= 2:
+            a, b = (int(x) for x in rng.choice(n, 2, replace=False))
+            obs.append(jq.build_parity_observable([a, b]))
+            obs.append(jq.PauliY(wires=b))
+        if with_dense and i % 7 == 3:
+            h = rng.normal(size=(2, 2)) + 1j * rng.normal(size=(2, 2))
+            obs.append(jq.Hermitian((h + h.conj().T) / 2, wires=int(rng.integers(n)), record=False))
+        inst.append((tape, n, obs))
+        refs.append((to_records(tape), n, obs_records(obs)))
+    return inst, refs
+
+
+def _check(bg, refs, ct, tol):
+    ev, g = bg.run()
+    torch.cuda.synchronize()
+    parts = bg.split(ev.cpu().numpy(), g.cpu().numpy())
+    o = 0
+    for (recs, n, obs), (e_i, g_i) in zip(refs, parts):
+        c = ct[o: o + len(obs)]
+        o += len(obs)
+        ev_ref, g_ref = O.adjoint_grad(recs, n, obs, ct=c)
+        np.testing.assert_allclose(e_i, ev_ref, atol=tol)
+        np.testing.assert_allclose(g_i, g_ref, atol=tol * max(1.0, np.abs(c).sum()))
+
+
+@pytest.mark.parametrize("dtype", [torch.complex64, torch.complex128])
+def test_batch_all_classes_match_oracle(dtype):
+    inst, refs = _instances(11, 30, 1, 14)
+    bg = jq.BatchedGradients(inst, dtype=dtype,
+                             config=dict(warp_max_qubits=5, cta_max_qubits=10, warp_threads=128, cta_threads=256))
+    cls = bg.classes
+    assert cls["warp"] > 0 and cls["cta"] > 0 and cls["tile"] > 0, cls
+    ct = np.random.default_rng(5).normal(size=bg.n_obs_total)
+    bg.set_cotangents(torch.tensor(ct))
+    _check(bg, refs, ct, TOL[dtype])
+    # replay of the captured graph, then new angles through the same graph
+    _check(bg, refs, ct, TOL[dtype])
+    rng = np.random.default_rng(9)
+    new = rng.uniform(0, 2 * np.pi, bg.n_angles_total)
+    bg.set_angles(torch.tensor(new))
+    o = 0
+    refs2 = []
+    for tape, n, obs in inst:
+        recs = to_records(tape)
+        out = []
+        for name, wires, params in recs:
+            # every float parameter is an angle, in recording order
+            k = sum(1 for p in params if isinstance(p, float))
+            assert k == len(params), (name, params)
+            newp = [float(v) for v in new[o: o + k]]
+            o += k
+            out.append((name, wires, newp))
+        refs2.append((out, n, obs_records(obs)))
+    _check(bg, refs2, ct, TOL[dtype])
+
+
+def test_batch_default_config_and_autotune():
+    inst, refs = _instances(12, 40, 2, 15, with_dense=False)
+    bg = jq.BatchedGradients(inst, dtype=torch.complex64)
+    ones = np.ones(bg.n_obs_total)
+    _check(bg, refs, ones, 1e-5)
+    chosen = bg.autotune()
+    assert chosen == bg.config
+    _check(bg, refs, ones, 1e-5)
+
+
+def test_batch_warp_only_small_circuits():
+    inst, refs = _instances(13, 64, 1, 6, with_dense=False)
+    bg = jq.BatchedGradients(inst, dtype=torch.complex128,
+                             config=dict(warp_max_qubits=6, cta_max_qubits=6, warp_threads=64, cta_threads=128))
+    assert bg.classes == {"warp": 64, "cta": 0, "tile": 0}
+    _check(bg, refs, np.ones(bg.n_obs_total), 1e-10)
