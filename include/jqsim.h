@@ -279,15 +279,19 @@ typedef struct jq_batch_config {
   int32_t warp_max_qubits; /* n <= this: one warp per instance, state in shared memory */
   int32_t cta_max_qubits;  /* n <= this: one CTA per instance, state in shared memory  */
   int32_t warp_threads;    /* threads per CTA of the warp-per-instance kernel (32..512) */
-  int32_t cta_threads;     /* threads per CTA of the CTA-per-instance kernel (64..512)  */
+  int32_t cta_threads;     /* threads per CTA of the CTA-per-instance and cluster kernels (64..512) */
+  int32_t cluster_bits;    /* n <= cta_max_qubits + cluster_bits (at most 3): one cluster of
+                              2^(n - cta_max_qubits) CTAs per instance, the state split over
+                              their shared memory; larger: batched tile passes             */
 } jq_batch_config;
 
-/* cfg NULL: defaults (complex64 9 / 13 qubits, complex128 8 / 12; 256 / 512 threads). */
+/* cfg NULL: defaults (complex64 9 / 13 qubits, complex128 8 / 12; 256 / 512 threads;
+ * cluster_bits 3). */
 JQ_API int jq_batch_build(jq_plan* const* plans, int n_plans, const int32_t* plan_of, int n_inst,
                           const jq_batch_config* cfg, jq_batch** out);
 JQ_API int jq_batch_free(jq_batch* batch);
 /* totals: angles (= gradient entries) and expectation values over all
- * instances; n_class[3] = instances in the warp, cta and tile classes. */
+ * instances; n_class[4] = instances in the warp, cta, tile and cluster classes. */
 JQ_API int jq_batch_info(const jq_batch* batch, int64_t* n_angles, int64_t* n_obs, int32_t* n_class,
                          jq_batch_config* cfg);
 /* Workspace for jq_batch_run under the current configuration and under

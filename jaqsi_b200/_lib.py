@@ -140,6 +140,7 @@ class JqBatchConfig(ctypes.Structure):
         ("cta_max_qubits", ctypes.c_int32),
         ("warp_threads", ctypes.c_int32),
         ("cta_threads", ctypes.c_int32),
+        ("cluster_bits", ctypes.c_int32),
     ]
 
     def as_dict(self) -> dict:

@@ -7,7 +7,9 @@ This is the gradient-workload form of the reference's batched execution
 :87-125), for circuits that do not share one structure.  Instances with the
 same structure share one plan.  Small instances run one per warp, mid-size
 ones one per CTA with the whole state in shared memory, larger ones as
-batched tile passes; the split is autotunable (:meth:`BatchedGradients.autotune`).
+batched tile passes or, up to three qubits above the
+per-CTA limit, one per thread-block cluster with the state split over the
+cluster's shared memory; the split is autotunable (:meth:`BatchedGradients.autotune`).
 
 Example::
 
@@ -131,9 +133,9 @@ class BatchedGradients:
     @property
     def classes(self) -> dict:
         """Instances per class under the current configuration."""
-        nc = (ctypes.c_int32 * 3)()
+        nc = (ctypes.c_int32 * 4)()
         L.check(self._lib.jq_batch_info(self.handle, None, None, nc, None))
-        return {"warp": nc[0], "cta": nc[1], "tile": nc[2]}
+        return {"warp": nc[0], "cta": nc[1], "tile": nc[2], "cluster": nc[3]}
 
     def set_config(self, **config) -> None:
         cfg = L.JqBatchConfig(**{**self.config, **config})

@@ -57,9 +57,9 @@ struct BatchArgs {
   const double* ct;      // per (instance, observable) cotangent; NULL: all ones
   double* expval;
   double* grad;
-  void* bmat_ws;         // per group slot: bmat_slot run-dtype complex
   double2* gacc_ws;      // per group slot: gacc_slot complex128
-  int64_t bmat_slot, gacc_slot;
+  int64_t bmat_slot;     // run-dtype complex of the block matrices per group (shared memory)
+  int64_t gacc_slot;
   int* counter;
 };
 
@@ -111,6 +111,10 @@ struct WarpRS {
   }
 };
 
+// Gradient partial sums: float for complex64 runs, double for complex128.
+template <typename C> struct AccT { using T = double; };
+template <> struct AccT<float2> { using T = float; };
+
 // Add the group's partial block cotangent (NV doubles per thread) into dst.
 template <bool WARP, int NV>
 __device__ __forceinline__ void gacc_add(double (&v)[NV], double* dst) {
@@ -123,31 +127,66 @@ __device__ __forceinline__ void gacc_add(double (&v)[NV], double* dst) {
   }
 }
 
+// acc += l * conj(p), in the accumulator type A
+template <typename A, typename C>
+__device__ __forceinline__ void acc_lconjp(A& re, A& im, C l, C p) {
+  re += static_cast<A>(l.x) * static_cast<A>(p.x) + static_cast<A>(l.y) * static_cast<A>(p.y);
+  im += static_cast<A>(l.y) * static_cast<A>(p.x) - static_cast<A>(l.x) * static_cast<A>(p.y);
+}
+
+template <bool WARP, int NV, typename A>
+__device__ __forceinline__ void gacc_add_acc(A (&v)[NV], double* dst) {
+  double d[NV];
+#pragma unroll
+  for (int e = 0; e < NV; ++e) d[e] = static_cast<double>(v[e]);
+  gacc_add<WARP, NV>(d, dst);
+}
+
 // Forward application of one block to the n-qubit state s.
+// gbase: global index bits above the n local ones (a cluster CTA's rank
+// bits; 0 for a state held whole); controls and diagonal rows may sit there.
 template <typename C>
-__device__ void bapply(C* s, int n, const BBlock& B, const C* bm, int lt, int gs) {
+__device__ void bapply(C* s, int n, const BBlock& B, const C* bm, int lt, int gs, uint32_t gbase = 0) {
   const int dim = 1 << n;
   const C* M = bm + B.mat_off;
   if (B.kind == BK_DIAG) {
     for (int j = lt; j < dim; j += gs) {
-      if ((static_cast<uint32_t>(j) & B.cmask) != B.cmask) continue;
-      const int r = (B.nt == 1) ? ((j >> B.tb0) & 1) : ((((j >> B.tb0) & 1) << 1) | ((j >> B.tb1) & 1));
+      const uint32_t gj = gbase | static_cast<uint32_t>(j);
+      if ((gj & B.cmask) != B.cmask) continue;
+      const int r = (B.nt == 1) ? ((gj >> B.tb0) & 1) : ((((gj >> B.tb0) & 1) << 1) | ((gj >> B.tb1) & 1));
       s[j] = cmul(M[r], s[j]);
     }
     return;
   }
   if (B.nt == 1) {
-    const int q = B.tb0;
-    for (int g = lt; g < (dim >> 1); g += gs) {
-      const int i0 = ins0(g, q);
-      if ((static_cast<uint32_t>(i0) & B.cmask) != B.cmask) continue;
-      const int i1 = i0 | (1 << q);
-      const C x = s[i0], y = s[i1];
-      if (B.kind == BK_PERM) {
-        if (B.perm & 1) { s[i0] = y; s[i1] = x; }
-      } else {
-        s[i0] = cfma(M[1], y, cmul(M[0], x));
-        s[i1] = cfma(M[3], y, cmul(M[2], x));
+    const int q = B.tb0, half = dim >> 1;
+    if (B.kind == BK_PERM && !(B.perm & 1)) return;
+    const C m0 = M[0], m1 = M[1], m2 = M[2], m3 = M[3];
+    // 4 pairs per thread at a time: every load before any store
+    for (int g0 = lt; g0 < half; g0 += 4 * gs) {
+      C x[4], y[4];
+      int i0[4];
+      bool ok[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int g = g0 + u * gs;
+        i0[u] = ins0(g, q);
+        ok[u] = g < half && ((gbase | static_cast<uint32_t>(i0[u])) & B.cmask) == B.cmask;
+        if (ok[u]) {
+          x[u] = s[i0[u]];
+          y[u] = s[i0[u] | (1 << q)];
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        if (!ok[u]) continue;
+        if (B.kind == BK_PERM) {
+          s[i0[u]] = y[u];
+          s[i0[u] | (1 << q)] = x[u];
+        } else {
+          s[i0[u]] = cfma(m1, y[u], cmul(m0, x[u]));
+          s[i0[u] | (1 << q)] = cfma(m3, y[u], cmul(m2, x[u]));
+        }
       }
     }
     return;
@@ -155,7 +194,7 @@ __device__ void bapply(C* s, int n, const BBlock& B, const C* bm, int lt, int gs
   const int lo = min(B.tb0, B.tb1), hi = max(B.tb0, B.tb1);
   for (int g = lt; g < (dim >> 2); g += gs) {
     const int i = ins0(ins0(g, lo), hi);
-    if ((static_cast<uint32_t>(i) & B.cmask) != B.cmask) continue;
+    if (((gbase | static_cast<uint32_t>(i)) & B.cmask) != B.cmask) continue;
     const int id[4] = {i, i | (1 << B.tb1), i | (1 << B.tb0), i | (1 << B.tb0) | (1 << B.tb1)};
     C a[4];
 #pragma unroll
@@ -174,39 +213,41 @@ __device__ void bapply(C* s, int n, const BBlock& B, const C* bm, int lt, int gs
 // Adjoint of one block: psi <- G^dagger psi, cotangent += lam psi^dagger
 // (psi after the un-apply), lam <- G^dagger lam.
 template <typename C, bool WARP>
-__device__ void badjoint(C* sp, C* sl, int n, const BBlock& B, const C* bm, double* ga, int lt, int gs) {
+__device__ void badjoint(C* sp, C* sl, int n, const BBlock& B, const C* bm, double* ga, int lt, int gs,
+                         uint32_t gbase = 0) {
   const int dim = 1 << n;
   const C* M = bm + B.mat_off;
   const bool grad = ga && B.grad_off >= 0;
   double* gdst = grad ? ga + 2 * B.grad_off : nullptr;
+  using A = typename AccT<C>::T;
   if (B.kind == BK_DIAG) {
-    double g[8];
+    A g[8];
 #pragma unroll
-    for (int e = 0; e < 8; ++e) g[e] = 0.0;
+    for (int e = 0; e < 8; ++e) g[e] = A(0);
     for (int j = lt; j < dim; j += gs) {
-      if ((static_cast<uint32_t>(j) & B.cmask) != B.cmask) continue;
-      const int r = (B.nt == 1) ? ((j >> B.tb0) & 1) : ((((j >> B.tb0) & 1) << 1) | ((j >> B.tb1) & 1));
+      const uint32_t gj = gbase | static_cast<uint32_t>(j);
+      if ((gj & B.cmask) != B.cmask) continue;
+      const int r = (B.nt == 1) ? ((gj >> B.tb0) & 1) : ((((gj >> B.tb0) & 1) << 1) | ((gj >> B.tb1) & 1));
       const C d = cconj(M[r]);
       const C p = cmul(d, sp[j]);
       const C l = sl[j];
       sp[j] = p;
       sl[j] = cmul(d, l);
-      const double2 v = cmul(to_d2(l), cconj(to_d2(p)));
 #pragma unroll
       for (int q = 0; q < 4; ++q)
-        if (q == r) { g[2 * q] += v.x; g[2 * q + 1] += v.y; }
+        if (q == r) acc_lconjp(g[2 * q], g[2 * q + 1], l, p);
     }
-    if (grad) gacc_add<WARP, 8>(g, gdst);
+    if (grad) gacc_add_acc<WARP, 8>(g, gdst);
     return;
   }
   if (B.nt == 1) {
     const int q = B.tb0;
-    double g[8];
+    A g[8];
 #pragma unroll
-    for (int e = 0; e < 8; ++e) g[e] = 0.0;
+    for (int e = 0; e < 8; ++e) g[e] = A(0);
     for (int gi = lt; gi < (dim >> 1); gi += gs) {
       const int i0 = ins0(gi, q);
-      if ((static_cast<uint32_t>(i0) & B.cmask) != B.cmask) continue;
+      if (((gbase | static_cast<uint32_t>(i0)) & B.cmask) != B.cmask) continue;
       const int i1 = i0 | (1 << q);
       const C x = sp[i0], y = sp[i1], u = sl[i0], w = sl[i1];
       if (B.kind == BK_PERM) {
@@ -218,23 +259,23 @@ __device__ void badjoint(C* sp, C* sl, int n, const BBlock& B, const C* bm, doub
       const C p0 = cfma(h01, y, cmul(h00, x)), p1 = cfma(h11, y, cmul(h10, x));
       sp[i0] = p0;
       sp[i1] = p1;
-      const double2 du = to_d2(u), dw = to_d2(w), d0 = cconj(to_d2(p0)), d1 = cconj(to_d2(p1));
-      const double2 g00 = cmul(du, d0), g01 = cmul(du, d1), g10 = cmul(dw, d0), g11 = cmul(dw, d1);
-      g[0] += g00.x; g[1] += g00.y; g[2] += g01.x; g[3] += g01.y;
-      g[4] += g10.x; g[5] += g10.y; g[6] += g11.x; g[7] += g11.y;
+      acc_lconjp(g[0], g[1], u, p0);
+      acc_lconjp(g[2], g[3], u, p1);
+      acc_lconjp(g[4], g[5], w, p0);
+      acc_lconjp(g[6], g[7], w, p1);
       sl[i0] = cfma(h01, w, cmul(h00, u));
       sl[i1] = cfma(h11, w, cmul(h10, u));
     }
-    if (grad) gacc_add<WARP, 8>(g, gdst);
+    if (grad) gacc_add_acc<WARP, 8>(g, gdst);
     return;
   }
   const int lo = min(B.tb0, B.tb1), hi = max(B.tb0, B.tb1);
-  double g[32];
+  A g[32];
 #pragma unroll
-  for (int e = 0; e < 32; ++e) g[e] = 0.0;
+  for (int e = 0; e < 32; ++e) g[e] = A(0);
   for (int gi = lt; gi < (dim >> 2); gi += gs) {
     const int i = ins0(ins0(gi, lo), hi);
-    if ((static_cast<uint32_t>(i) & B.cmask) != B.cmask) continue;
+    if (((gbase | static_cast<uint32_t>(i)) & B.cmask) != B.cmask) continue;
     const int id[4] = {i, i | (1 << B.tb1), i | (1 << B.tb0), i | (1 << B.tb0) | (1 << B.tb1)};
     C a[4], b[4];
 #pragma unroll
@@ -258,15 +299,9 @@ __device__ void badjoint(C* sp, C* sl, int n, const BBlock& B, const C* bm, doub
       sp[id[r]] = acc;
     }
 #pragma unroll
-    for (int r = 0; r < 4; ++r) {
-      const double2 lr = to_d2(b[r]);
+    for (int r = 0; r < 4; ++r)
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const double2 v = cmul(lr, cconj(to_d2(p[q])));
-        g[2 * (4 * r + q)] += v.x;
-        g[2 * (4 * r + q) + 1] += v.y;
-      }
-    }
+      for (int q = 0; q < 4; ++q) acc_lconjp(g[2 * (4 * r + q)], g[2 * (4 * r + q) + 1], b[r], p[q]);
 #pragma unroll
     for (int r = 0; r < 4; ++r) {
       C acc = cmul(cconj(M[r]), b[0]);
@@ -275,11 +310,11 @@ __device__ void badjoint(C* sp, C* sl, int n, const BBlock& B, const C* bm, doub
       sl[id[r]] = acc;
     }
   }
-  if (grad) gacc_add<WARP, 32>(g, gdst);
+  if (grad) gacc_add_acc<WARP, 32>(g, gdst);
 }
 
 template <typename R, bool WARP>
-__global__ void __launch_bounds__(512) k_batch(BatchArgs a) {
+__global__ void __launch_bounds__(512, 1) k_batch(BatchArgs a) {
   using C = typename CplxT<R>::T;
   extern __shared__ __align__(16) unsigned char smem[];
   const int gs = WARP ? 32 : static_cast<int>(blockDim.x);
@@ -287,12 +322,15 @@ __global__ void __launch_bounds__(512) k_batch(BatchArgs a) {
   const int gid = WARP ? static_cast<int>(threadIdx.x >> 5) : 0;
   const int lt = WARP ? static_cast<int>(threadIdx.x & 31) : static_cast<int>(threadIdx.x);
   const int dmax = 1 << a.nmax;
+  // shared memory: psi and lambda of every group, then the block matrices
+  // of every group's current instance, then reduction scratch
   C* sp = reinterpret_cast<C*>(smem) + static_cast<int64_t>(gid) * 2 * dmax;
   C* sl = sp + dmax;
-  double* red = reinterpret_cast<double*>(reinterpret_cast<C*>(smem) + static_cast<int64_t>(ngroups) * 2 * dmax);
-  int* snext = reinterpret_cast<int*>(red + 32);
+  C* bm = reinterpret_cast<C*>(smem) + static_cast<int64_t>(ngroups) * 2 * dmax + gid * a.bmat_slot;
+  double* red =
+      reinterpret_cast<double*>(reinterpret_cast<C*>(smem) + static_cast<int64_t>(ngroups) * (2 * dmax + a.bmat_slot));
+  int* snext = reinterpret_cast<int*>(red + 64);
   const int64_t slot = static_cast<int64_t>(blockIdx.x) * ngroups + gid;
-  C* bm = static_cast<C*>(a.bmat_ws) + slot * a.bmat_slot;
   double2* gacc = a.gacc_ws + slot * a.gacc_slot;
   for (;;) {
     int k;
@@ -351,6 +389,386 @@ __global__ void __launch_bounds__(512) k_batch(BatchArgs a) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// cluster class: one instance on a cluster of CL CTAs; CTA `rank` holds the
+// amplitudes whose top log2(CL) index bits equal rank (its local slice of
+// 2^L, L = n - log2 CL, for psi and for lambda).  Blocks whose targets are
+// local bits run as in the single-CTA kernel (controls and diagonal rows
+// may use the rank bits); a dense or permutation block with a target among
+// the rank bits reads its sibling amplitudes from the other CTAs' shared
+// memory (distributed shared memory), computes this CTA's new values into
+// a global scratch slice, waits for the cluster, then writes them back.
+// ---------------------------------------------------------------------------
+struct ClusterArgs {
+  BatchArgs a;
+  int lbits;          // L: local index bits per CTA
+  void* xs_ws;        // per CTA: 2 * 2^L run-dtype complex exchange scratch
+};
+
+__device__ __forceinline__ bool bdist(const BBlock& B, int lbits) {
+  return B.kind != BK_DIAG && (B.tb0 >= lbits || (B.nt == 2 && B.tb1 >= lbits));
+}
+
+// Global index of sibling c (target bits set to c) of global index g.
+__device__ __forceinline__ uint32_t bsib(const BBlock& B, uint32_t g, int c) {
+  if (B.nt == 1) return (g & ~(1u << B.tb0)) | (static_cast<uint32_t>(c & 1) << B.tb0);
+  g &= ~((1u << B.tb0) | (1u << B.tb1));
+  return g | (static_cast<uint32_t>((c >> 1) & 1) << B.tb0) | (static_cast<uint32_t>(c & 1) << B.tb1);
+}
+
+__device__ __forceinline__ int brow(const BBlock& B, uint32_t g) {
+  return B.nt == 1 ? static_cast<int>((g >> B.tb0) & 1) : static_cast<int>((((g >> B.tb0) & 1) << 1) | ((g >> B.tb1) & 1));
+}
+
+// Adjoint of a block with a target among the rank bits (NT targets): new
+// psi and lambda of this CTA's rows into xs (psi) and xs + 2^L (lambda), the
+// block cotangent into gacc.  Every sibling row is read from the CTA that
+// holds it; the caller syncs the cluster before and after.
+template <typename C, int NT, int CL>
+__device__ __forceinline__ void cl_adj_dist(cooperative_groups::cluster_group& cluster, const BBlock& B, const C* bm,
+                                            C* sp, C* sl, C* xs, double2* gacc, int lb, uint32_t gbase, int lt,
+                                            int gs) {
+  using A = typename AccT<C>::T;
+  constexpr int ND = 1 << NT;
+  const int nloc = 1 << lb;
+  const C* M = bm + B.mat_off;
+  const bool grad = B.grad_off >= 0;
+  A gs2[2 * ND * ND];
+#pragma unroll
+  for (int e = 0; e < 2 * ND * ND; ++e) gs2[e] = A(0);
+  for (int j = lt; j < nloc; j += gs) {
+    const uint32_t g = gbase | static_cast<uint32_t>(j);
+    if ((g & B.cmask) != B.cmask) continue;
+    const int r = brow(B, g);
+    C vp[ND], vl[ND];
+#pragma unroll
+    for (int c = 0; c < ND; ++c) {
+      const uint32_t gc = bsib(B, g, c);
+      vp[c] = cluster.map_shared_rank(sp, gc >> lb)[gc & (nloc - 1)];
+      vl[c] = cluster.map_shared_rank(sl, gc >> lb)[gc & (nloc - 1)];
+    }
+    if (B.kind == BK_PERM) {
+      // inverse permutation: new[p[r']] = old[r'] (exactly one r' has p[r'] = r)
+      C op = vp[0], ol = vl[0];
+#pragma unroll
+      for (int c = 1; c < ND; ++c)
+        if (((B.perm >> (2 * c)) & 3) == r) { op = vp[c]; ol = vl[c]; }
+      xs[j] = op;
+      xs[nloc + j] = ol;
+      continue;
+    }
+    // psi' = G^dagger psi on every row of the group (rows other CTAs own too)
+    C np[ND];
+#pragma unroll
+    for (int c = 0; c < ND; ++c) {
+      C acc = cmul(cconj(M[c]), vp[0]);
+#pragma unroll
+      for (int c2 = 1; c2 < ND; ++c2) acc = cfma(cconj(M[c2 * ND + c]), vp[c2], acc);
+      np[c] = acc;
+    }
+    C nl = cmul(cconj(M[r]), vl[0]);
+#pragma unroll
+    for (int c2 = 1; c2 < ND; ++c2) nl = cfma(cconj(M[c2 * ND + r]), vl[c2], nl);
+    C mine = np[0], lr = vl[0];
+#pragma unroll
+    for (int c = 1; c < ND; ++c)
+      if (c == r) { mine = np[c]; lr = vl[c]; }
+    xs[j] = mine;
+    xs[nloc + j] = nl;
+    if (grad) {
+#pragma unroll
+      for (int rr = 0; rr < ND; ++rr) {
+        if (rr != r) continue;
+#pragma unroll
+        for (int c = 0; c < ND; ++c) {
+          // lambda_r conj(psi'_c)
+          gs2[2 * (rr * ND + c)] += static_cast<A>(lr.x) * np[c].x + static_cast<A>(lr.y) * np[c].y;
+          gs2[2 * (rr * ND + c) + 1] += static_cast<A>(lr.y) * np[c].x - static_cast<A>(lr.x) * np[c].y;
+        }
+      }
+    }
+  }
+  if (grad) {
+    double gd[2 * ND * ND];
+#pragma unroll
+    for (int e = 0; e < 2 * ND * ND; ++e) gd[e] = static_cast<double>(gs2[e]);
+    gacc_add<false, 2 * ND * ND>(gd, reinterpret_cast<double*>(gacc) + 2 * B.grad_off);
+  }
+}
+
+// Fast path of a one-target block on a rank bit (complex64, 16 amplitudes
+// per thread): the partner CTA's amplitudes at this thread's own local
+// indices are the only ones needed, so they move as 8 independent 16-byte
+// DSMEM loads per vector into registers between the two cluster barriers.
+template <int CL>
+__device__ __forceinline__ void cl_fwd_fast(cooperative_groups::cluster_group& cluster, const BBlock& B,
+                                            const float2* M, float2* sp, int lb, uint32_t rank, int lt, int gs) {
+  const uint32_t pr = rank ^ (1u << (B.tb0 - lb));
+  const int mybit = static_cast<int>((rank >> (B.tb0 - lb)) & 1);
+  const uint32_t gbase = rank << lb;
+  const float4* rsp = reinterpret_cast<const float4*>(cluster.map_shared_rank(sp, pr));
+  float4* own = reinterpret_cast<float4*>(sp);
+  float4 pv[8];
+  cluster.sync();  // partner values final
+#pragma unroll
+  for (int k = 0; k < 8; ++k) pv[k] = rsp[lt + k * gs];
+  cluster.sync();  // every CTA holds what it needs
+  const bool perm = B.kind == BK_PERM;
+  const bool swap = perm && (B.perm & 1);
+  const float2 a = mybit ? M[3] : M[0], b = mybit ? M[2] : M[1];  // new own = a own + b partner
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    const int idx = lt + k * gs;
+    float4 o = own[idx];
+    const float4 q = pv[k];
+    float2 x0 = make_float2(o.x, o.y), x1 = make_float2(o.z, o.w);
+    const float2 y0 = make_float2(q.x, q.y), y1 = make_float2(q.z, q.w);
+    const uint32_t g0 = gbase | static_cast<uint32_t>(2 * idx);
+    const bool c0 = (g0 & B.cmask) == B.cmask, c1 = ((g0 | 1u) & B.cmask) == B.cmask;
+    if (perm) {
+      if (swap && c0) x0 = y0;
+      if (swap && c1) x1 = y1;
+    } else {
+      if (c0) x0 = cfma(b, y0, cmul(a, x0));
+      if (c1) x1 = cfma(b, y1, cmul(a, x1));
+    }
+    own[idx] = make_float4(x0.x, x0.y, x1.x, x1.y);
+  }
+  __syncthreads();
+}
+
+template <int CL>
+__device__ __forceinline__ void cl_adj_fast(cooperative_groups::cluster_group& cluster, const BBlock& B,
+                                            const float2* M, float2* sp, float2* sl, double2* gacc, int lb,
+                                            uint32_t rank, int lt, int gs) {
+  const uint32_t pr = rank ^ (1u << (B.tb0 - lb));
+  const int mybit = static_cast<int>((rank >> (B.tb0 - lb)) & 1);
+  const uint32_t gbase = rank << lb;
+  const float4* rsp = reinterpret_cast<const float4*>(cluster.map_shared_rank(sp, pr));
+  const float4* rsl = reinterpret_cast<const float4*>(cluster.map_shared_rank(sl, pr));
+  float4* ownp = reinterpret_cast<float4*>(sp);
+  float4* ownl = reinterpret_cast<float4*>(sl);
+  float4 pp[8], pl[8];
+  cluster.sync();
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    pp[k] = rsp[lt + k * gs];
+    pl[k] = rsl[lt + k * gs];
+  }
+  cluster.sync();
+  const bool perm = B.kind == BK_PERM;
+  const bool swap = perm && (B.perm & 1);
+  const bool grad = !perm && B.grad_off >= 0;
+  // rows: b = mybit (own), 1 - b (partner).  G^dagger[c][c2] = conj(M[c2][c]).
+  const int bo = mybit, bp = 1 - mybit;
+  float g[8];
+#pragma unroll
+  for (int e = 0; e < 8; ++e) g[e] = 0.0f;
+  auto step = [&](float2& xo, float2 xp, float2& lo, float2 lp) {
+    if (perm) {
+      if (swap) { xo = xp; lo = lp; }
+      return;
+    }
+    // psi_c for c = bo (own) and bp (partner); psi'_c = sum_c2 conj(M[c2][c]) psi_c2
+    float2 ps[2], ls[2];
+    ps[bo] = xo; ps[bp] = xp;
+    ls[bo] = lo; ls[bp] = lp;
+    const float2 n0 = cfma(cconj(M[2]), ps[1], cmul(cconj(M[0]), ps[0]));
+    const float2 n1 = cfma(cconj(M[3]), ps[1], cmul(cconj(M[1]), ps[0]));
+    const float2 lnew = bo ? cfma(cconj(M[3]), ls[1], cmul(cconj(M[1]), ls[0]))
+                           : cfma(cconj(M[2]), ls[1], cmul(cconj(M[0]), ls[0]));
+    if (grad) {
+      // lambda_bo conj(psi'_c)
+      const float2 l = lo;
+      g[4 * bo + 0] += l.x * n0.x + l.y * n0.y;
+      g[4 * bo + 1] += l.y * n0.x - l.x * n0.y;
+      g[4 * bo + 2] += l.x * n1.x + l.y * n1.y;
+      g[4 * bo + 3] += l.y * n1.x - l.x * n1.y;
+    }
+    xo = bo ? n1 : n0;
+    lo = lnew;
+  };
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    const int idx = lt + k * gs;
+    const float4 op = ownp[idx], ol = ownl[idx], qp = pp[k], ql = pl[k];
+    float2 x0 = make_float2(op.x, op.y), x1 = make_float2(op.z, op.w);
+    float2 l0 = make_float2(ol.x, ol.y), l1 = make_float2(ol.z, ol.w);
+    const uint32_t g0 = gbase | static_cast<uint32_t>(2 * idx);
+    if ((g0 & B.cmask) == B.cmask) step(x0, make_float2(qp.x, qp.y), l0, make_float2(ql.x, ql.y));
+    if (((g0 | 1u) & B.cmask) == B.cmask) step(x1, make_float2(qp.z, qp.w), l1, make_float2(ql.z, ql.w));
+    ownp[idx] = make_float4(x0.x, x0.y, x1.x, x1.y);
+    ownl[idx] = make_float4(l0.x, l0.y, l1.x, l1.y);
+  }
+  if (grad) gacc_add_acc<false, 8>(g, reinterpret_cast<double*>(gacc) + 2 * B.grad_off);
+  __syncthreads();
+}
+
+template <typename R, int CL>
+__global__ void __launch_bounds__(512, 1) k_batch_cluster(ClusterArgs ca) {
+  using C = typename CplxT<R>::T;
+  namespace cg = cooperative_groups;
+  cg::cluster_group cluster = cg::this_cluster();
+  const BatchArgs& a = ca.a;
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int lb = ca.lbits, nloc = 1 << lb;
+  const int gs = static_cast<int>(blockDim.x), lt = static_cast<int>(threadIdx.x);
+  const uint32_t rank = cluster.block_rank();
+  C* sp = reinterpret_cast<C*>(smem);
+  C* sl = sp + nloc;
+  C* bm = sl + nloc;                                    // block matrices of the instance
+  double* red = reinterpret_cast<double*>(bm + a.bmat_slot);  // 32 doubles
+  double* spart = red + 32;                            // 32 per-observable partial sums
+  int* snext = reinterpret_cast<int*>(spart + 32);
+  C* rp[CL];
+  C* rl[CL];
+#pragma unroll
+  for (int r = 0; r < CL; ++r) {
+    rp[r] = cluster.map_shared_rank(sp, r);
+    rl[r] = cluster.map_shared_rank(sl, r);
+  }
+  const int64_t cid = blockIdx.x / CL;
+  double2* gacc = a.gacc_ws + cid * a.gacc_slot;
+  C* xs = static_cast<C*>(ca.xs_ws) + static_cast<int64_t>(blockIdx.x) * 2 * nloc;
+  const uint32_t gbase = rank << lb;
+  for (;;) {
+    if (rank == 0 && lt == 0) snext[0] = atomicAdd(a.counter, 1);
+    cluster.sync();
+    const int k = *cluster.map_shared_rank(snext, 0);
+    cluster.sync();
+    if (k >= a.n_order) break;
+    const BInst I = a.inst[a.order[k]];
+    const BPlan P = a.plans[I.plan];
+    const double* ang = a.angles + I.angle_off;
+    const BBlock* BB = a.bblk + P.blk_off;
+    for (int b = lt; b < P.nblocks; b += gs)
+      prep_block<R>(a.dblk[P.blk_off + b], a.prims, a.ops, ang, nullptr, a.cpool, bm, nullptr);
+    if (rank == 0)
+      for (int e = lt; e < P.grad_stride; e += gs) gacc[e] = make_double2(0.0, 0.0);
+    for (int j = lt; j < nloc; j += gs) sp[j] = cmake<C>((gbase | static_cast<uint32_t>(j)) == 0 ? 1.0 : 0.0, 0.0);
+    cluster.sync();
+    // forward
+    for (int b = 0; b < P.nblocks; ++b) {
+      const BBlock B = BB[b];
+      if (!bdist(B, lb)) {
+        bapply<C>(sp, lb, B, bm, lt, gs, gbase);
+        __syncthreads();
+        continue;
+      }
+      if constexpr (sizeof(C) == 8) {
+        if (B.nt == 1 && nloc == 16 * gs) {
+          cl_fwd_fast<CL>(cluster, B, bm + B.mat_off, sp, lb, rank, lt, gs);
+          continue;
+        }
+      }
+      cluster.sync();  // every CTA's earlier writes are final
+      const C* M = bm + B.mat_off;
+      const int nd = 1 << B.nt;
+      // U elements per thread at a time: all sibling loads (local or remote)
+      // issue before any use; the new values go to the lambda slice, which
+      // the forward sweep does not use yet
+      constexpr int U = 2;
+      for (int j0 = lt; j0 < nloc; j0 += U * gs) {
+        C v[U][4];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          const int j = j0 + u * gs;
+          const uint32_t g = gbase | static_cast<uint32_t>(j);
+          if (j < nloc && (g & B.cmask) == B.cmask) {
+#pragma unroll
+            for (int c = 0; c < 4; ++c)
+              if (c < nd) {
+                const uint32_t gc = bsib(B, g, c);
+                v[u][c] = cluster.map_shared_rank(sp, gc >> lb)[gc & (nloc - 1)];
+              }
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          const int j = j0 + u * gs;
+          const uint32_t g = gbase | static_cast<uint32_t>(j);
+          if (j >= nloc || (g & B.cmask) != B.cmask) continue;
+          const int r = brow(B, g);
+          C out;
+          if (B.kind == BK_PERM) {
+            const int src = (B.perm >> (2 * r)) & 3;
+            out = v[u][0];
+#pragma unroll
+            for (int c = 1; c < 4; ++c)
+              if (c == src) out = v[u][c];
+          } else {
+            out = cmul(M[r * nd], v[u][0]);
+#pragma unroll
+            for (int c = 1; c < 4; ++c)
+              if (c < nd) out = cfma(M[r * nd + c], v[u][c], out);
+          }
+          sl[j] = out;
+        }
+      }
+      cluster.sync();  // every read of the old values is done
+      for (int j = lt; j < nloc; j += gs)
+        if (((gbase | static_cast<uint32_t>(j)) & B.cmask) == B.cmask) sp[j] = sl[j];
+      __syncthreads();
+    }
+    cluster.sync();
+    // expectation values (partial sums per CTA, added by rank 0) and lambda
+    for (int j = lt; j < nloc; j += gs) sl[j] = cmake<C>(0.0, 0.0);
+    for (int o = 0; o < P.n_obs; ++o) {
+      const DevObs ob = a.obs[P.obs_off + o];
+      const double w = 2.0 * (a.ct ? a.ct[I.out_off + o] : 1.0) * ob.coeff;
+      double part = 0.0;
+      for (int j = lt; j < nloc; j += gs) {
+        const uint32_t g = gbase | static_cast<uint32_t>(j);
+        const uint32_t gx = g ^ static_cast<uint32_t>(ob.x_mask);
+        const double sign = (__popc(gx & static_cast<uint32_t>(ob.z_mask)) & 1) ? -1.0 : 1.0;
+        const double2 v = mul_iy(ob.n_y, to_d2(rp[gx >> lb][gx & (nloc - 1)]));
+        const double2 pj = to_d2(sp[j]);
+        part += sign * (pj.x * v.x + pj.y * v.y);
+        const double2 l = to_d2(sl[j]);
+        sl[j] = cmake<C>(l.x + w * sign * v.x, l.y + w * sign * v.y);
+      }
+      const double tot = gsum<false>(part, red);
+      if (lt == 0) spart[o] = tot;
+    }
+    cluster.sync();
+    if (rank == 0 && lt < P.n_obs) {
+      double tot = 0.0;
+      for (int r = 0; r < CL; ++r) tot += *cluster.map_shared_rank(spart + lt, r);
+      a.expval[I.out_off + lt] = a.obs[P.obs_off + lt].coeff * tot;
+    }
+    // adjoint
+    for (int b = P.nblocks - 1; b >= 0; --b) {
+      const BBlock B = BB[b];
+      if (!bdist(B, lb)) {
+        badjoint<C, false>(sp, sl, lb, B, bm, reinterpret_cast<double*>(gacc), lt, gs, gbase);
+        __syncthreads();
+        continue;
+      }
+      if constexpr (sizeof(C) == 8) {
+        if (B.nt == 1 && nloc == 16 * gs) {
+          cl_adj_fast<CL>(cluster, B, bm + B.mat_off, sp, sl, gacc, lb, rank, lt, gs);
+          continue;
+        }
+      }
+      cluster.sync();
+      if (B.nt == 1) cl_adj_dist<C, 1, CL>(cluster, B, bm, sp, sl, xs, gacc, lb, gbase, lt, gs);
+      else cl_adj_dist<C, 2, CL>(cluster, B, bm, sp, sl, xs, gacc, lb, gbase, lt, gs);
+      cluster.sync();
+      for (int j = lt; j < nloc; j += gs)
+        if (((gbase | static_cast<uint32_t>(j)) & B.cmask) == B.cmask) {
+          sp[j] = xs[j];
+          sl[j] = xs[nloc + j];
+        }
+      __syncthreads();
+    }
+    cluster.sync();  // every cotangent contribution is in
+    for (int b = static_cast<int>(rank) * gs + lt; b < P.nblocks; b += CL * gs)
+      chain_block(a.dblk[P.blk_off + b], a.prims, a.ops, ang, nullptr, a.cpool, gacc, nullptr, a.grad + I.angle_off,
+                  nullptr);
+    cluster.sync();  // the cotangent slot and block matrices are free again
+  }
+}
+
 // gather / scatter between the batch's instance layout and a plan group's
 // dense (instance, entry) layout
 __global__ void k_gather_rows(const double* src, const int64_t* src_off, int rows, int width, double* dst) {
@@ -406,6 +824,7 @@ struct jq_batch {
   void* d_tile_off = nullptr;  // per tile group: angle offsets then output offsets of its instances
   // classes under the current configuration
   std::vector<int32_t> order_warp, order_cta;
+  std::vector<int32_t> order_cl[3];   // cluster class, clusters of 2, 4, 8 CTAs
   struct TileGroup {
     int plan;
     std::vector<int32_t> members;
@@ -414,14 +833,15 @@ struct jq_batch {
   std::vector<TileGroup> tiles;
   int nmax_warp = 0, nmax_cta = 0;
   int64_t bmat_slot = 0, gacc_slot = 0, slots_warp = 0;
+  int64_t bs_warp = 0, bs_cta = 0, bs_cl = 0;  // block-matrix elements per group in shared memory
   // workspace layout
-  size_t ws_total = 0, ws_counter = 0, ws_bmat = 0, ws_gacc = 0;
+  size_t ws_total = 0, ws_counter = 0, ws_gacc = 0, ws_cl_xs = 0;
   std::vector<size_t> ws_tile;  // per tile group: angles, ct, outs, grads, state, fwd ws, adj ws
   std::vector<size_t> ws_tile_fwd, ws_tile_adj;
   // side streams and the captured graph
-  cudaStream_t side[2] = {nullptr, nullptr};
+  cudaStream_t side[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
   cudaStream_t cap = nullptr;   // the graph is captured on this stream
-  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
   cudaGraphExec_t graph = nullptr;
   const void* graph_key[7] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
   int sm_count = 0;
@@ -429,6 +849,15 @@ struct jq_batch {
 
 namespace jq {
 namespace {
+
+// Shared memory of a warp / cta / cluster kernel: per group psi, lambda
+// (2^nmax each) and the block matrices (bs run-dtype complex, even).
+size_t batch_smem(int nmax, int groups, int elem, int64_t bs) {
+  return static_cast<size_t>(groups) * (2 * (static_cast<size_t>(1) << nmax) + static_cast<size_t>(bs)) * elem +
+         64 * 8 + 16;
+}
+
+int64_t even(int64_t x) { return (x + 1) & ~static_cast<int64_t>(1); }
 
 int64_t plan_cost(const jq_batch* b, int p) {
   return (static_cast<int64_t>(1) << b->n_of_plan[p]) * std::max(1, b->bplans[p].nblocks);
@@ -447,14 +876,20 @@ int plan_class(const jq_batch* b, int p, const jq_batch_config& c) {
   for (const DevObs& o : pl->obs)
     if (o.kind != JQ_OBS_PAULI) smem_ok = false;
   if (!smem_ok) return 2;
-  if (n <= c.warp_max_qubits) return 0;
-  if (n <= c.cta_max_qubits) return 1;
+  const int elem = b->dtype == JQ_C64 ? 8 : 16;
+  const int64_t bs = even(pl->bmat_stride);
+  const size_t budget = 227 * 1024;
+  if (n <= c.warp_max_qubits && batch_smem(c.warp_max_qubits, c.warp_threads / 32, elem, bs) <= budget) return 0;
+  if (n <= c.cta_max_qubits && batch_smem(c.cta_max_qubits, 1, elem, bs) <= budget) return 1;
+  if (n > c.cta_max_qubits && n <= c.cta_max_qubits + std::min(c.cluster_bits, 3) && pl->obs.size() <= 32 &&
+      n <= 31 && batch_smem(c.cta_max_qubits, 1, elem, bs) <= budget)
+    return 3;
   return 2;
 }
 
-size_t batch_smem(int nmax, int groups, int elem) {
-  return static_cast<size_t>(groups) * 2 * (static_cast<size_t>(1) << nmax) * elem + 32 * 8 + 16;
-}
+// Clusters per SM slot of the cluster class (one 2^L slice per CTA).
+int cluster_index(int n, int cta_max) { return n - cta_max - 1; }  // 0: 2 CTAs, 1: 4, 2: 8
+
 
 int batch_classify(jq_batch* b, bool dry = false);
 
@@ -477,6 +912,7 @@ int batch_classify(jq_batch* b, bool dry) {
   const jq_batch_config& c = b->cfg;
   b->order_warp.clear();
   b->order_cta.clear();
+  for (auto& v : b->order_cl) v.clear();
   b->tiles.clear();
   b->nmax_warp = b->nmax_cta = 0;
   std::vector<int> cls(b->plans.size());
@@ -493,6 +929,8 @@ int batch_classify(jq_batch* b, bool dry) {
     } else if (cls[p] == 1) {
       b->order_cta.push_back(i);
       b->nmax_cta = std::max(b->nmax_cta, b->n_of_plan[p]);
+    } else if (cls[p] == 3) {
+      b->order_cl[cluster_index(b->n_of_plan[p], c.cta_max_qubits)].push_back(i);
     } else {
       if (tile_of[p] < 0) {
         tile_of[p] = static_cast<int>(b->tiles.size());
@@ -507,16 +945,17 @@ int batch_classify(jq_batch* b, bool dry) {
   };
   std::sort(b->order_warp.begin(), b->order_warp.end(), by_cost);
   std::sort(b->order_cta.begin(), b->order_cta.end(), by_cost);
+  for (auto& v : b->order_cl) std::sort(v.begin(), v.end(), by_cost);
+  b->bs_warp = b->bs_cta = b->bs_cl = 0;
+  for (size_t p = 0; p < b->plans.size(); ++p) {
+    const int64_t bs = even(b->plans[p]->bmat_stride);
+    if (cls[p] == 0) b->bs_warp = std::max(b->bs_warp, bs);
+    if (cls[p] == 1) b->bs_cta = std::max(b->bs_cta, bs);
+    if (cls[p] == 3) b->bs_cl = std::max(b->bs_cl, bs);
+  }
   const int elem = b->dtype == JQ_C64 ? 8 : 16;
   const int wgroups = c.warp_threads / 32;
-  if (!b->order_warp.empty() && batch_smem(b->nmax_warp, wgroups, elem) > 227 * 1024) {
-    set_error("warp-class shared memory above 227 KB: lower warp_max_qubits or warp_threads");
-    return JQ_EINVAL;
-  }
-  if (!b->order_cta.empty() && batch_smem(b->nmax_cta, 1, elem) > 227 * 1024) {
-    set_error("cta-class shared memory above 227 KB: lower cta_max_qubits");
-    return JQ_EINVAL;
-  }
+
   if (dry) {
     // workspace size only (same arithmetic as below)
     int64_t bs = 1, gsl = 1;
@@ -525,8 +964,10 @@ int batch_classify(jq_batch* b, bool dry) {
       bs = std::max<int64_t>(bs, b->plans[p]->bmat_stride);
       gsl = std::max<int64_t>(gsl, b->plans[p]->grad_stride);
     }
-    const int64_t slots = static_cast<int64_t>(b->sm_count) * 16 * (std::max(1, wgroups) + 1);
-    size_t off = 256 + align256(static_cast<size_t>(slots) * bs * elem) + align256(static_cast<size_t>(slots) * gsl * 16);
+    const int64_t slots = static_cast<int64_t>(b->sm_count) * (16 * (std::max(1, wgroups) + 1) + 3);
+    size_t off = 256 + align256(static_cast<size_t>(slots) * gsl * 16);
+    (void)bs;
+    off += align256(static_cast<size_t>(3) * b->sm_count * 2 * (static_cast<size_t>(1) << c.cta_max_qubits) * elem);
     for (auto& tg : b->tiles) {
       const jq_plan* pl = b->plans[tg.plan];
       const int nb = static_cast<int>(tg.members.size());
@@ -542,6 +983,7 @@ int batch_classify(jq_batch* b, bool dry) {
   // order table and tile-group offset table
   std::vector<int32_t> order(b->order_warp);
   order.insert(order.end(), b->order_cta.begin(), b->order_cta.end());
+  for (auto& v : b->order_cl) order.insert(order.end(), v.begin(), v.end());
   if (order.empty()) order.push_back(0);
   std::vector<int64_t> toff;
   for (auto& tg : b->tiles) {
@@ -571,14 +1013,16 @@ int batch_classify(jq_batch* b, bool dry) {
   // the two shared-memory kernels run concurrently: warp-class slots first,
   // then one slot per CTA of the cta-class kernel
   b->slots_warp = static_cast<int64_t>(b->sm_count) * 16 * std::max(1, wgroups);
-  const int64_t slots = b->slots_warp + static_cast<int64_t>(b->sm_count) * 16;
+  // then one slot per CTA of the cta-class kernel, then 3 x sm_count for the
+  // three cluster launches (at most one cluster-class CTA per SM each)
+  const int64_t slots = b->slots_warp + static_cast<int64_t>(b->sm_count) * 16 + 3LL * b->sm_count;
   size_t off = 0;
   b->ws_counter = off;
   off += 256;
-  b->ws_bmat = off;
-  off += align256(static_cast<size_t>(slots) * bs * elem);
   b->ws_gacc = off;
   off += align256(static_cast<size_t>(slots) * gsl * 16);
+  b->ws_cl_xs = off;
+  off += align256(static_cast<size_t>(3) * b->sm_count * 2 * (static_cast<size_t>(1) << c.cta_max_qubits) * elem);
   b->ws_tile.clear();
   b->ws_tile_fwd.clear();
   b->ws_tile_adj.clear();
@@ -627,14 +1071,13 @@ int batch_launch_smem(jq_batch* b, bool warp, const double* angles, const double
   a.expval = expval;
   a.grad = grad;
   const int64_t slot0 = warp ? 0 : b->slots_warp;
-  a.bmat_ws = w + b->ws_bmat + static_cast<size_t>(slot0 * b->bmat_slot) * elem;
   a.gacc_ws = reinterpret_cast<double2*>(w + b->ws_gacc) + slot0 * b->gacc_slot;
-  a.bmat_slot = b->bmat_slot;
+  a.bmat_slot = warp ? b->bs_warp : b->bs_cta;
   a.gacc_slot = b->gacc_slot;
   a.counter = reinterpret_cast<int*>(w + b->ws_counter) + (warp ? 0 : 1);
   const int threads = warp ? b->cfg.warp_threads : b->cfg.cta_threads;
   const int groups = warp ? threads / 32 : 1;
-  const size_t smem = batch_smem(a.nmax, groups, elem);
+  const size_t smem = batch_smem(a.nmax, groups, elem, a.bmat_slot);
   auto kern = warp ? k_batch<R, true> : k_batch<R, false>;
   JQ_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
   int per_sm = 0;
@@ -648,6 +1091,70 @@ int batch_launch_smem(jq_batch* b, bool warp, const double* angles, const double
   const int grid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(need, static_cast<int64_t>(b->sm_count) * per_sm)));
   kern<<<grid, threads, smem, st>>>(a);
   JQ_CUDA(cudaGetLastError());
+  return JQ_OK;
+}
+
+template <typename R, int CL>
+int batch_launch_cluster(jq_batch* b, int ci, const double* angles, const double* ct, double* expval, double* grad,
+                         char* w, cudaStream_t st) {
+  const std::vector<int32_t>& ord = b->order_cl[ci];
+  if (ord.empty()) return JQ_OK;
+  const int elem = static_cast<int>(sizeof(typename CplxT<R>::T));
+  const int lbits = b->cfg.cta_max_qubits;
+  ClusterArgs ca;
+  BatchArgs& a = ca.a;
+  size_t before = b->order_warp.size() + b->order_cta.size();
+  for (int i = 0; i < ci; ++i) before += b->order_cl[i].size();
+  a.plans = static_cast<const BPlan*>(b->d_plans);
+  a.inst = static_cast<const BInst*>(b->d_inst);
+  a.order = static_cast<const int32_t*>(b->d_order) + before;
+  a.n_order = static_cast<int>(ord.size());
+  a.nmax = lbits;
+  a.bblk = static_cast<const BBlock*>(b->d_bblk);
+  a.dblk = static_cast<const DevBlock*>(b->d_dblk);
+  a.prims = static_cast<const DevPrim*>(b->d_prims);
+  a.ops = static_cast<const DevOp*>(b->d_ops);
+  a.cpool = static_cast<const double2*>(b->d_cpool);
+  a.obs = static_cast<const DevObs*>(b->d_obs);
+  a.angles = angles;
+  a.ct = ct;
+  a.expval = expval;
+  a.grad = grad;
+  // CTA slots (block matrices) and cluster slots (cotangents) after the
+  // warp- and cta-class slots; sm_count of each per cluster launch
+  const int64_t slot0 = b->slots_warp + static_cast<int64_t>(b->sm_count) * 16 + static_cast<int64_t>(ci) * b->sm_count;
+  a.gacc_ws = reinterpret_cast<double2*>(w + b->ws_gacc) + slot0 * b->gacc_slot;
+  a.bmat_slot = b->bs_cl;
+  a.gacc_slot = b->gacc_slot;
+  a.counter = reinterpret_cast<int*>(w + b->ws_counter) + 2 + ci;
+  ca.lbits = lbits;
+  ca.xs_ws = w + b->ws_cl_xs + static_cast<size_t>(ci) * b->sm_count * 2 * (static_cast<size_t>(1) << lbits) * elem;
+  const int threads = b->cfg.cta_threads;
+  const size_t smem = batch_smem(lbits, 1, elem, a.bmat_slot);
+  auto kern = k_batch_cluster<R, CL>;
+  JQ_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+  cudaLaunchConfig_t cfg = {};
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = CL;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.blockDim = dim3(threads, 1, 1);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cfg.gridDim = dim3(CL * 16, 1, 1);
+  int max_clusters = 0;
+  JQ_CUDA(cudaOccupancyMaxActiveClusters(&max_clusters, kern, &cfg));
+  if (max_clusters < 1) {
+    set_error("batch cluster kernel does not fit with this configuration");
+    return JQ_EINVAL;
+  }
+  const int64_t cap = std::max<int64_t>(1, std::min<int64_t>(max_clusters, b->sm_count / CL));
+  const int64_t nclusters = std::max<int64_t>(1, std::min<int64_t>(static_cast<int64_t>(ord.size()), cap));
+  cfg.gridDim = dim3(static_cast<unsigned>(nclusters * CL), 1, 1);
+  JQ_CUDA(cudaLaunchKernelEx(&cfg, kern, ca));
   return JQ_OK;
 }
 
@@ -706,18 +1213,21 @@ int batch_enqueue(jq_batch* b, const double* angles, const double* ct, double* e
   JQ_CUDA(cudaMemsetAsync(w + b->ws_counter, 0, 256, st));
   if (b->n_angles_total > 0) JQ_CUDA(cudaMemsetAsync(grad, 0, static_cast<size_t>(b->n_angles_total) * 8, st));
   JQ_CUDA(cudaEventRecord(b->ev[0], st));
-  JQ_CUDA(cudaStreamWaitEvent(b->side[0], b->ev[0], 0));
-  JQ_CUDA(cudaStreamWaitEvent(b->side[1], b->ev[0], 0));
+  for (int i = 0; i < 5; ++i) JQ_CUDA(cudaStreamWaitEvent(b->side[i], b->ev[0], 0));
   int rc;
-  // tile groups on side stream 0, warp class on side stream 1, cta class on st
+  // largest work first: clusters of 8, 4, 2 CTAs on side streams 2..4, tile
+  // groups on side stream 0, warp class on side stream 1, cta class on st
+  if ((rc = batch_launch_cluster<R, 8>(b, 2, angles, ct, expval, grad, w, b->side[2]))) return rc;
+  if ((rc = batch_launch_cluster<R, 4>(b, 1, angles, ct, expval, grad, w, b->side[3]))) return rc;
+  if ((rc = batch_launch_cluster<R, 2>(b, 0, angles, ct, expval, grad, w, b->side[4]))) return rc;
   for (size_t g = 0; g < b->tiles.size(); ++g)
     if ((rc = batch_tile_group<R>(b, g, angles, ct, expval, grad, w, b->side[0]))) return rc;
   if ((rc = batch_launch_smem<R>(b, true, angles, ct, expval, grad, w, b->side[1]))) return rc;
   if ((rc = batch_launch_smem<R>(b, false, angles, ct, expval, grad, w, st))) return rc;
-  JQ_CUDA(cudaEventRecord(b->ev[1], b->side[0]));
-  JQ_CUDA(cudaEventRecord(b->ev[2], b->side[1]));
-  JQ_CUDA(cudaStreamWaitEvent(st, b->ev[1], 0));
-  JQ_CUDA(cudaStreamWaitEvent(st, b->ev[2], 0));
+  for (int i = 0; i < 5; ++i) {
+    JQ_CUDA(cudaEventRecord(b->ev[1 + i], b->side[i]));
+    JQ_CUDA(cudaStreamWaitEvent(st, b->ev[1 + i], 0));
+  }
   return JQ_OK;
 }
 

@@ -7,6 +7,7 @@
 // block of the pass that acts inside the tile, and writes the tile back.  One
 // pass therefore replaces the reference's one-XLA-loop-per-entry
 // (jaqsi/simulation.py:400-409) for all the blocks it holds.
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -1119,7 +1120,7 @@ __global__ void __launch_bounds__(512, 1) k_tile_bwd(const typename CplxT<R>::T*
 // Inner matrix (or diagonal) of one block of one instance into bm (the
 // instance's block matrices); `sc` is the instance's scratch (k > 2 blocks).
 template <typename R>
-__device__ void prep_block(const DevBlock& blk, const DevPrim* __restrict__ prims, const DevOp* __restrict__ ops,
+__device__ __noinline__ void prep_block(const DevBlock& blk, const DevPrim* __restrict__ prims, const DevOp* __restrict__ ops,
                            const double* ang, const double2* mt, const double2* __restrict__ cpool,
                            typename CplxT<R>::T* bm, double2* sc) {
   using C = typename CplxT<R>::T;
@@ -1176,7 +1177,7 @@ __global__ void k_prep(const DevBlock* __restrict__ blocks, int nblocks, const D
 // Chain rule of one block of one instance: block cotangent (gacc: the
 // instance's accumulators) -> per-prim cotangents -> angle / matrix gradients
 // (ga_out / gm_out: the instance's gradient rows, accumulated atomically).
-__device__ void chain_block(const DevBlock& blk, const DevPrim* __restrict__ prims, const DevOp* __restrict__ ops,
+__device__ __noinline__ void chain_block(const DevBlock& blk, const DevPrim* __restrict__ prims, const DevOp* __restrict__ ops,
                             const double* ang, const double2* mt, const double2* __restrict__ cpool,
                             const double2* gacc, double2* sc, double* ga_out, double2* gm_out) {
   if (blk.grad_off < 0) return;
@@ -2318,13 +2319,14 @@ jq_batch_config batch_default_config(int dtype) {
   c.cta_max_qubits = dtype == JQ_C64 ? 13 : 12;
   c.warp_threads = 256;
   c.cta_threads = 512;
+  c.cluster_bits = 3;
   return c;
 }
 
 bool batch_config_ok(const jq_batch_config& c) {
   return c.warp_max_qubits >= 0 && c.warp_max_qubits <= 12 && c.cta_max_qubits >= 0 && c.cta_max_qubits <= 14 &&
          c.warp_threads >= 32 && c.warp_threads <= 512 && (c.warp_threads % 32) == 0 && c.cta_threads >= 64 &&
-         c.cta_threads <= 512 && (c.cta_threads % 32) == 0;
+         c.cta_threads <= 512 && (c.cta_threads % 32) == 0 && c.cluster_bits >= 0 && c.cluster_bits <= 3;
 }
 
 std::vector<jq_batch_config> batch_candidates(const jq_batch* b) {
@@ -2338,9 +2340,9 @@ std::vector<jq_batch_config> batch_candidates(const jq_batch* b) {
     for (int cm : (c64 ? cmax_c64 : cmax_c128))
       for (int wt : {128, 256})
         for (int ct : {256, 512}) {
-          jq_batch_config c{wm, cm, wt, ct};
+          jq_batch_config c{wm, cm, wt, ct, 3};
           const int elem = c64 ? 8 : 16;
-          if (batch_smem(wm, wt / 32, elem) > 227 * 1024) continue;
+          if (batch_smem(wm, wt / 32, elem, 0) > 227 * 1024) continue;
           out.push_back(c);
         }
   }
@@ -2724,10 +2726,10 @@ int jq_batch_build(jq_plan* const* plans, int n_plans, const int32_t* plan_of, i
     set_error("jq_batch_build: upload of the batch tables failed");
     return JQ_ECUDA;
   }
-  for (int i = 0; i < 2; ++i)
+  for (int i = 0; i < 5; ++i)
     if (cudaStreamCreateWithFlags(&b->side[i], cudaStreamNonBlocking) != cudaSuccess) return JQ_ECUDA;
   if (cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking) != cudaSuccess) return JQ_ECUDA;
-  for (int i = 0; i < 4; ++i)
+  for (int i = 0; i < 6; ++i)
     if (cudaEventCreateWithFlags(&b->ev[i], cudaEventDisableTiming) != cudaSuccess) return JQ_ECUDA;
   if (int rc = batch_classify(b.get())) return rc;
   *out = b.release();
@@ -2741,10 +2743,10 @@ int jq_batch_free(jq_batch* b) {
                   b->d_order, b->d_tile_off};
   for (void* p : bufs)
     if (p) cudaFree(p);
-  for (int i = 0; i < 2; ++i)
+  for (int i = 0; i < 5; ++i)
     if (b->side[i]) cudaStreamDestroy(b->side[i]);
   if (b->cap) cudaStreamDestroy(b->cap);
-  for (int i = 0; i < 4; ++i)
+  for (int i = 0; i < 6; ++i)
     if (b->ev[i]) cudaEventDestroy(b->ev[i]);
   delete b;
   return JQ_OK;
@@ -2763,6 +2765,7 @@ int jq_batch_info(const jq_batch* b, int64_t* n_angles, int64_t* n_obs, int32_t*
     int32_t t = 0;
     for (const auto& tg : b->tiles) t += static_cast<int32_t>(tg.members.size());
     n_class[2] = t;
+    n_class[3] = static_cast<int32_t>(b->order_cl[0].size() + b->order_cl[1].size() + b->order_cl[2].size());
   }
   if (cfg) *cfg = b->cfg;
   return JQ_OK;

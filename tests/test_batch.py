@@ -1,8 +1,8 @@
 """Batched uneven instances (jq_batch): expectation values and full adjoint
 gradients of many independent circuits in one CUDA-graph launch, against the
-oracle's per-instance adjoint gradient.  Instances span all three classes
-(one per warp, one per CTA, batched tile passes) by choosing the class
-thresholds explicitly.
+oracle's per-instance adjoint gradient.  Instances span all four classes
+(one per warp, one per CTA, one per thread-block cluster of 2-8 CTAs, batched
+tile passes) by choosing the class thresholds explicitly.
 """
 import numpy as np
 import pytest
@@ -54,11 +54,12 @@ def _check(bg, refs, ct, tol):
 
 @pytest.mark.parametrize("dtype", [torch.complex64, torch.complex128])
 def test_batch_all_classes_match_oracle(dtype):
-    inst, refs = _instances(11, 30, 1, 14)
+    inst, refs = _instances(11, 36, 1, 14)
     bg = jq.BatchedGradients(inst, dtype=dtype,
-                             config=dict(warp_max_qubits=5, cta_max_qubits=10, warp_threads=128, cta_threads=256))
+                             config=dict(warp_max_qubits=5, cta_max_qubits=9, warp_threads=128, cta_threads=256,
+                                         cluster_bits=3))
     cls = bg.classes
-    assert cls["warp"] > 0 and cls["cta"] > 0 and cls["tile"] > 0, cls
+    assert cls["warp"] > 0 and cls["cta"] > 0 and cls["tile"] > 0 and cls["cluster"] > 0, cls
     ct = np.random.default_rng(5).normal(size=bg.n_obs_total)
     bg.set_cotangents(torch.tensor(ct))
     _check(bg, refs, ct, TOL[dtype])
@@ -97,5 +98,37 @@ def test_batch_warp_only_small_circuits():
     inst, refs = _instances(13, 64, 1, 6, with_dense=False)
     bg = jq.BatchedGradients(inst, dtype=torch.complex128,
                              config=dict(warp_max_qubits=6, cta_max_qubits=6, warp_threads=64, cta_threads=128))
-    assert bg.classes == {"warp": 64, "cta": 0, "tile": 0}
+    assert bg.classes == {"warp": 64, "cta": 0, "tile": 0, "cluster": 0}
     _check(bg, refs, np.ones(bg.n_obs_total), 1e-10)
+
+
+def test_batch_cluster_class_all_cluster_sizes():
+    """Rot + CX-ring instances at 11, 12 and 13 qubits with a 10-qubit CTA
+    slice: clusters of 2, 4 and 8 CTAs, against the oracle.  64 threads per
+    CTA takes the vectorised exchange for one-target blocks on rank bits
+    (16 amplitudes a thread, complex64); 128 threads the general one."""
+    rng = np.random.default_rng(21)
+    inst, refs = [], []
+    for i in range(18):
+        n = 11 + i % 3
+        d = int(rng.integers(2, 5))
+        ang = rng.uniform(0, 2 * np.pi, (d, n, 3))
+        with jq.recording() as tape:
+            for l in range(d):
+                for w in range(n):
+                    jq.Rot(float(ang[l, w, 0]), float(ang[l, w, 1]), float(ang[l, w, 2]), wires=w)
+                for w in range(n):
+                    jq.CX(wires=[w, (w + 1) % n])
+            jq.CRY(0.3 + 0.1 * i, wires=[0, n - 1])
+            jq.RZZ(0.7, wires=[1, n - 2])
+            jq.SWAP(wires=[0, 5])
+        obs = [jq.PauliZ(0), jq.PauliX(1), jq.build_parity_observable([0, n - 1]), jq.PauliY(n - 1)]
+        inst.append((tape, n, obs))
+        refs.append((to_records(tape), n, obs_records(obs)))
+    for dtype in (torch.complex64, torch.complex128):
+        for threads in (64, 128):
+            bg = jq.BatchedGradients(inst, dtype=dtype,
+                                     config=dict(warp_max_qubits=0, cta_max_qubits=10, warp_threads=64,
+                                                 cta_threads=threads, cluster_bits=3))
+            assert bg.classes["cluster"] == 18, bg.classes
+            _check(bg, refs, np.ones(bg.n_obs_total), TOL[dtype])
