@@ -212,6 +212,175 @@ def _config(args, p_ref, p_ours):
     }
 
 
+def batched_adjoint_leg(args, dev, steps, warmup):
+    """4096 uneven instances (qubits uniform 6..16, 10..40 layers of Rot on
+    every wire + CX ring, independent seeded angles, <Z_0>): expectation value
+    plus the full adjoint gradient of every instance in one CUDA-graph launch,
+    against the plain per-circuit forward kernel driven by parameter shift
+    (2 forwards per angle + 1, every shifted set of an instance in one batched
+    forward call) on a seeded sample of the instances, scaled to the workload."""
+    import torch
+
+    import jaqsi_b200 as jq
+    from jaqsi_b200 import _lib as L
+    from jaqsi_b200 import simulation as sim
+
+    rng = np.random.default_rng(4)
+    count = args.batch_instances
+    shapes = [(int(rng.integers(6, 17)), int(rng.integers(10, 41))) for _ in range(count)]
+    angles = [rng.uniform(0, 2 * np.pi, (d, n, 3)) for n, d in shapes]
+
+    def record(n, d, ang):
+        a = ang.tolist()
+        with jq.recording() as tape:
+            for l in range(d):
+                for w in range(n):
+                    jq.Rot(a[l][w][0], a[l][w][1], a[l][w][2], wires=w)
+                for w in range(n):
+                    jq.CX(wires=[w, (w + 1) % n])
+        return tape
+
+    t0 = time.perf_counter()
+    tapes = [record(n, d, a) for (n, d), a in zip(shapes, angles)]
+    obs = [jq.PauliZ(0)]
+    t1 = time.perf_counter()
+    bg = jq.BatchedGradients([(t, n, obs) for t, (n, _) in zip(tapes, shapes)], dtype=torch.complex64)
+    print(f"[bench] batched leg: record {t1 - t0:.1f} s, build {time.perf_counter() - t1:.1f} s", file=sys.stderr,
+          flush=True)
+    stream = torch.cuda.current_stream()
+    for _ in range(max(1, warmup)):
+        bg.run()
+    torch.cuda.synchronize()
+    ts = []
+    for _ in range(steps):
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        bg.run()
+        b.record(stream)
+        b.synchronize()
+        ts.append(a.elapsed_time(b))
+    ms = statistics.median(ts)
+    ev, grad = bg.run()
+    grad64 = grad.detach().cpu().numpy().copy()
+    parts = bg.split(ev.detach().cpu().numpy(), grad64)
+
+    # parameter-shift baseline and gradient error on a seeded sample
+    srng = np.random.default_rng(40)
+    sample = sorted(srng.choice(count, size=min(args.shift_sample, count), replace=False).tolist())
+    shift_ms = 0.0
+    work_sample = 0
+    work_total = sum(6 * n * d + 1 for n, d in shapes)
+    max_err = 0.0
+    ps_err = 0.0
+    ref = jq.BatchedGradients([(tapes[i], shapes[i][0], obs) for i in sample], dtype=torch.complex128)
+    _, g128 = ref.run()
+    g128 = g128.detach().cpu().numpy()
+    off = 0
+    for k, i in enumerate(sample):
+        n, d = shapes[i]
+        na = 3 * n * d
+        max_err = max(max_err, float(np.abs(parts[i][1] - g128[off: off + na]).max()))
+        off += na
+        lw = sim.lower_tape(tapes[i], n)
+        specs, okey = sim._lower_obs(obs, n)
+        plan = sim.get_plan(lw, specs, okey, n, L.JQ_STATEVECTOR, torch.complex64, {"jit": -1})
+        base = torch.tensor([float(v) for v in lw.angles], dtype=torch.float64, device=dev)
+        sets = base.repeat(2 * na + 1, 1)
+        idx = torch.arange(na, device=dev)
+        sets[1 + idx, idx] += np.pi / 2
+        sets[1 + na + idx, idx] -= np.pi / 2
+        nb = sets.shape[0]
+        state = torch.empty((nb, plan.state_elems), dtype=torch.complex64, device=dev)
+        out = torch.empty((nb, plan.n_obs), dtype=torch.float64, device=dev)
+        wsb = plan.workspace_bytes(nb, 0)
+        ws = torch.empty(max(wsb, 1), dtype=torch.uint8, device=dev)
+        vp = ctypes.c_void_p
+        sp = vp(stream.cuda_stream)
+
+        def fwd():
+            L.check(plan._lib.jq_forward(plan.handle, nb, vp(sets.data_ptr()), None, None, 0, L.JQ_OUT_EXPVAL,
+                                         vp(state.data_ptr()), vp(out.data_ptr()), vp(ws.data_ptr()), wsb, sp))
+            # gradient = (f(+) - f(-)) / 2 per angle
+            return (out[1: 1 + na, 0] - out[1 + na:, 0]) * 0.5
+
+        fwd()
+        torch.cuda.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        gps = fwd()
+        b.record(stream)
+        b.synchronize()
+        shift_ms += a.elapsed_time(b)
+        work_sample += 2 * na + 1
+        ps_err = max(ps_err, float(np.abs(gps.cpu().numpy() - g128[off - na: off]).max()))
+        del state, ws
+    shift_total_ms = shift_ms * work_total / max(work_sample, 1)
+    return {
+        "workload": f"{count} instances, qubits uniform 6..16, 10..40 layers of Rot on every wire + CX ring, "
+                    f"<Z_0>, complex64, seeded (numpy default_rng(4))",
+        "grads_per_s": count / (ms * 1e-3), "ms_per_step": ms, "steps": steps,
+        "classes": bg.classes, "config": bg.config,
+        "param_shift_grads_per_s": count / (shift_total_ms * 1e-3),
+        "param_shift_ms_scaled": shift_total_ms,
+        "param_shift_sample": f"{len(sample)} seeded instances timed (one batched jq_forward of the 2P+1 shifted "
+                              f"sets each), scaled by forwards {work_total}/{work_sample}",
+        "speedup_vs_param_shift": shift_total_ms / ms,
+        "max_abs_grad_err_vs_c128": max_err,
+        "param_shift_max_abs_grad_err_vs_c128": ps_err,
+        "gpu_launches_per_step": "1 CUDA graph",
+    }
+
+
+def adjoint_20q_leg(dev, steps):
+    """20 qubits, 50 layers of Rot on every wire + CX(i, i + r mod n) with
+    r = (layer mod 19) + 1, 3000 seeded angles, sum_i Z_i Z_(i+1): one
+    forward + adjoint gradient per step through jq_forward / jq_adjoint."""
+    import torch
+
+    import jaqsi_b200 as jq
+    from jaqsi_b200 import _lib as L
+    from jaqsi_b200 import simulation as sim
+
+    n, layers = 20, 50
+    ang = np.random.default_rng(3).uniform(0, 2 * np.pi, (layers, n, 3))
+    a = torch.tensor(ang, requires_grad=True)
+    with jq.recording() as tape:
+        for l in range(layers):
+            for w in range(n):
+                jq.Rot(a[l, w, 0], a[l, w, 1], a[l, w, 2], wires=w)
+            r = (l % 19) + 1
+            for w in range(n):
+                jq.CX(wires=[w, (w + r) % n])
+    obs = [jq.build_parity_observable([i, i + 1]) for i in range(n - 1)]
+    out = {}
+    for dt, name in ((torch.complex64, "c64"), (torch.complex128, "c128")):
+        def step():
+            a.grad = None
+            ev = sim.simulate_and_measure(tape, n, "expval", obs, False, dtype=dt)
+            ev.sum().backward()
+            return ev
+
+        step()
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(steps):
+            t0 = torch.cuda.Event(enable_timing=True)
+            t1 = torch.cuda.Event(enable_timing=True)
+            t0.record()
+            step()
+            t1.record()
+            t1.synchronize()
+            ts.append(t0.elapsed_time(t1))
+        out[name] = (statistics.median(ts), a.grad.detach().clone())
+    err = float((out["c64"][1] - out["c128"][1]).abs().max())
+    return {"workload": "20 qubits, 50 layers Rot + CX range (layer mod 19)+1, 3000 angles, sum Z_iZ_(i+1)",
+            "ms_per_grad_c64": out["c64"][0], "grads_per_s_c64": 1e3 / out["c64"][0],
+            "ms_per_grad_c128": out["c128"][0], "max_abs_grad_err_c64_vs_c128": err,
+            "timed": "forward + adjoint through the public API (simulate_and_measure + backward)"}
+
+
 def ours_arm(args):
     import torch
     import torch.distributed as dist
@@ -299,10 +468,13 @@ def ours_arm(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
+    t_warm = time.perf_counter()
     for _ in range(args.warmup):
         fwd()
         sweep()
     barrier()
+    print(f"[bench] 24-qubit plan warm-up (incl. specialisation) {time.perf_counter() - t_warm:.1f} s",
+          file=sys.stderr, flush=True)
     with Clocks(local) as clk:
         step_ms = max_over_ranks(timed(fwd, args.steps))
         barrier()
@@ -355,6 +527,13 @@ def ours_arm(args):
         "clocks": clk.summary(),
         "expval_sum": float(ev.sum()),
     }
+    if not args.no_batch:
+        t0 = time.perf_counter()
+        result["batched_adjoint"] = batched_adjoint_leg(args, dev, max(3, args.steps // 2), args.warmup)
+        t1 = time.perf_counter()
+        result["adjoint_20q"] = adjoint_20q_leg(dev, max(3, args.steps // 2))
+        print(f"[bench] batched leg {t1 - t0:.1f} s, 20-qubit adjoint leg {time.perf_counter() - t1:.1f} s",
+              file=sys.stderr, flush=True)
     if rank == 0 and world == 1 and not args.no_cpu:
         s, _, cores, threads, cev = cpu_reference(args.sample_layers, args.dtype)
         result["cpu_baseline"] = {
@@ -380,6 +559,10 @@ def main():
     ap.add_argument("--sample-layers", type=int, default=2)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--tile-bits", type=int, default=0, help="override the forward tile size (qubits per CTA)")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched-adjoint and 20-qubit adjoint legs")
+    ap.add_argument("--batch-instances", type=int, default=4096)
+    ap.add_argument("--shift-sample", type=int, default=24,
+                    help="instances whose parameter-shift baseline is timed and scaled")
     args = ap.parse_args()
     if args.impl == "reference":
         return reference_arm(args)

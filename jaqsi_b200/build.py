@@ -38,7 +38,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
         "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
         "--expt-relaxed-constexpr", "-I", os.path.join(HERE, "..", "include"),
         *[os.path.join(CSRC, s) for s in SOURCES],
-        "-o", LIB + ".tmp", "-lcudart", "-ldl",
+        "-o", LIB + ".tmp", "-lcudart", "-ldl", "-lpthread",
     ]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")

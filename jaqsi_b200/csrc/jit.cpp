@@ -23,6 +23,7 @@
 #include <mutex>
 #include <sstream>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "jit.h"
@@ -801,7 +802,8 @@ bool jit_pass_eligible(const Schedule& s, int p) {
 // Kernel text of every eligible pass (forward, or adjoint when `adjoint`);
 // identical texts share one kernel.  Appends to `all`, names kernels prefix + k.
 void emit_kernels(const jq_plan* plan, const Schedule& s, bool adjoint, const char* prefix, std::ostringstream& all,
-                  std::vector<int>* kernel_of, std::vector<std::string>* names) {
+                  std::vector<int>* kernel_of, std::vector<std::string>* names,
+                  std::vector<std::string>* bodies = nullptr) {
   kernel_of->assign(s.passes.size(), -1);
   std::vector<std::string> texts;
   for (int p = 0; p < static_cast<int>(s.passes.size()); ++p) {
@@ -821,6 +823,7 @@ void emit_kernels(const jq_plan* plan, const Schedule& s, bool adjoint, const ch
       std::string body = text;
       body.replace(body.find("@KERNEL@"), 8, name);
       all << body;
+      if (bodies) bodies->push_back(body);
     }
     (*kernel_of)[p] = k;
   }
@@ -846,52 +849,81 @@ int jit_build(const jq_plan* plan, const Schedule& s, JitModule* out) {
     return JQ_EUNSUPPORTED;
   }
   std::ostringstream all;
-  all << kPrelude;
   std::vector<int> kernel_of, akernel_of;
-  std::vector<std::string> names, anames;
-  emit_kernels(plan, s, false, "jqk", all, &kernel_of, &names);
+  std::vector<std::string> names, anames, bodies;
+  emit_kernels(plan, s, false, "jqk", all, &kernel_of, &names, &bodies);
   const bool adj = plan_wants_adjoint(plan);
-  if (adj) emit_kernels(plan, s, true, "jqa", all, &akernel_of, &anames);
-  const std::string src = all.str();
+  if (adj) emit_kernels(plan, s, true, "jqa", all, &akernel_of, &anames, &bodies);
   out->fn.assign(s.passes.size(), nullptr);
   out->afn.assign(s.passes.size(), nullptr);
-  out->module = nullptr;
+  out->modules.clear();
   out->mc = nullptr;
   out->gt = nullptr;
   out->mc_off.assign(s.passes.size(), 0);
   out->gt_off.assign(s.passes.size(), 0);
   if (names.empty()) return JQ_OK;
-  nvrtcProgram prog;
-  if (g_nvrtc.create(&prog, src.c_str(), "jq_plan.cu", 0, nullptr, nullptr) != NVRTC_SUCCESS) {
-    set_error("nvrtcCreateProgram failed");
-    return JQ_EUNSUPPORTED;
+  // The kernels compile as independent NVRTC programs on parallel host
+  // threads (a large plan has hundreds of straight-line kernels); each
+  // chunk is loaded as its own module.
+  const int nk = static_cast<int>(bodies.size());
+  int hw = static_cast<int>(std::thread::hardware_concurrency());
+  if (hw <= 0) hw = 4;
+  const int nchunk = std::max(1, std::min(std::min(hw, 32), (nk + 1) / 2));
+  std::vector<std::string> srcs(nchunk, std::string(kPrelude));
+  std::vector<int> chunk_of(nk);
+  for (int k = 0; k < nk; ++k) {
+    chunk_of[k] = k % nchunk;
+    srcs[k % nchunk] += bodies[k];
   }
-  const char* opts[] = {"--gpu-architecture=sm_100a", "--std=c++17", "-default-device"};
-  const nvrtcResult cr = g_nvrtc.compile(prog, 3, opts);
-  if (cr != NVRTC_SUCCESS) {
-    size_t n = 0;
-    g_nvrtc.log_size(prog, &n);
-    std::string log(n, '\0');
-    g_nvrtc.log(prog, &log[0]);
+  std::vector<std::vector<char>> bins(nchunk);
+  std::vector<std::string> errs(nchunk);
+  auto compile = [&](int c) {
+    nvrtcProgram prog;
+    if (g_nvrtc.create(&prog, srcs[c].c_str(), "jq_plan.cu", 0, nullptr, nullptr) != NVRTC_SUCCESS) {
+      errs[c] = "nvrtcCreateProgram failed";
+      return;
+    }
+    const char* opts[] = {"--gpu-architecture=sm_100a", "--std=c++17", "-default-device"};
+    if (g_nvrtc.compile(prog, 3, opts) != NVRTC_SUCCESS) {
+      size_t n = 0;
+      g_nvrtc.log_size(prog, &n);
+      std::string log(n, '\0');
+      g_nvrtc.log(prog, &log[0]);
+      errs[c] = "NVRTC compile of the plan failed: " + log.substr(0, 2000);
+      g_nvrtc.destroy(&prog);
+      return;
+    }
+    size_t nbin = 0;
+    g_nvrtc.cubin_size(prog, &nbin);
+    bins[c].resize(nbin);
+    g_nvrtc.cubin(prog, bins[c].data());
     g_nvrtc.destroy(&prog);
-    set_error("NVRTC compile of the plan failed: " + log.substr(0, 2000));
-    return JQ_EUNSUPPORTED;
+  };
+  {
+    std::vector<std::thread> th;
+    for (int c = 1; c < nchunk; ++c) th.emplace_back(compile, c);
+    compile(0);
+    for (auto& t : th) t.join();
   }
-  size_t nbin = 0;
-  g_nvrtc.cubin_size(prog, &nbin);
-  std::vector<char> bin(nbin);
-  g_nvrtc.cubin(prog, bin.data());
-  g_nvrtc.destroy(&prog);
-  CUmodule mod;
-  if (g_drv.module_load(&mod, bin.data()) != CUDA_SUCCESS) {
-    set_error("cuModuleLoadData failed for the specialised plan");
-    return JQ_ECUDA;
+  for (int c = 0; c < nchunk; ++c)
+    if (!errs[c].empty()) {
+      set_error(errs[c]);
+      return JQ_EUNSUPPORTED;
+    }
+  for (int c = 0; c < nchunk; ++c) {
+    CUmodule mod;
+    if (g_drv.module_load(&mod, bins[c].data()) != CUDA_SUCCESS) {
+      set_error("cuModuleLoadData failed for the specialised plan");
+      return JQ_ECUDA;
+    }
+    out->modules.push_back(mod);
   }
-  out->module = mod;
-  auto lookup = [&](const std::vector<std::string>& nm, std::vector<void*>* fk) -> int {
+  // kernel k of the forward list is body k; adjoint kernel k is body |names| + k
+  auto lookup = [&](const std::vector<std::string>& nm, int base, std::vector<void*>* fk) -> int {
     fk->assign(nm.size(), nullptr);
     for (size_t k = 0; k < nm.size(); ++k) {
       CUfunction f;
+      CUmodule mod = static_cast<CUmodule>(out->modules[chunk_of[base + static_cast<int>(k)]]);
       if (g_drv.get_function(&f, mod, nm[k].c_str()) != CUDA_SUCCESS) {
         set_error("cuModuleGetFunction failed for " + nm[k]);
         return JQ_ECUDA;
@@ -902,7 +934,7 @@ int jit_build(const jq_plan* plan, const Schedule& s, JitModule* out) {
     return JQ_OK;
   };
   std::vector<void*> fk, ak;
-  if (lookup(names, &fk) || lookup(anames, &ak)) return JQ_ECUDA;
+  if (lookup(names, 0, &fk) || lookup(anames, static_cast<int>(names.size()), &ak)) return JQ_ECUDA;
   // per-pass matrix staging tables
   std::vector<int32_t> mc;
   // per-pass gradient flush tables: (shared accumulator offset, block
@@ -945,14 +977,15 @@ int jit_build(const jq_plan* plan, const Schedule& s, JitModule* out) {
 }
 
 void jit_free(JitModule* m) {
-  if (m && m->module && g_drv.ok) g_drv.module_unload(static_cast<CUmodule>(m->module));
+  if (m && g_drv.ok)
+    for (void* mod : m->modules) g_drv.module_unload(static_cast<CUmodule>(mod));
   if (m && m->mc) cudaFree(m->mc);
   if (m && m->gt) cudaFree(m->gt);
   if (m) {
     m->mc = nullptr;
     m->gt = nullptr;
     m->afn.clear();
-    m->module = nullptr;
+    m->modules.clear();
     m->fn.clear();
   }
 }

@@ -11,7 +11,7 @@
 namespace jq {
 
 struct JitModule {
-  void* module = nullptr;       // CUmodule
+  std::vector<void*> modules;   // CUmodule per NVRTC program (kernels compile in parallel chunks)
   std::vector<void*> fn;        // CUfunction per pass (nullptr: interpreter)
   std::vector<void*> afn;       // adjoint CUfunction per pass (unitary statevector plans)
   void* mc = nullptr;           // device int32 matrix staging tables
