@@ -178,6 +178,10 @@ Schedule schedule(const std::vector<HostBlock>& blocks, const std::vector<DevBlo
       if ((blocked | 0) == all_bits) break;
     }
     while (cursor < nblk && done[cursor]) ++cursor;
+    // Fill the tile up to t_max with the lowest free bits: the same ops then
+    // run on fewer, larger tiles (longer contiguous runs, fewer per-tile
+    // reductions), which matters most for one-block passes.
+    for (int bit = 0; bit < nb && popcount64(S) < t_max; ++bit) S |= 1ULL << bit;
     PassDesc pd;
     std::memset(&pd, 0, sizeof(pd));
     int t = 0;
