@@ -40,6 +40,11 @@ sys.path.insert(0, ROOT)
 
 METRIC = "adjoint grads/sec (batched) vs plain GPU sim at ≤1e-5 err; gate-pass HBM GB/s"
 N_QUBITS, LAYERS, SEED = 24, 20, 2
+# DRAM bytes per launch of the specialised tile pass, from one ncu capture
+# (--set full, 2 launches of the 24-qubit complex64 sweep): reads 134.3 MB
+# (the whole state once) + writes 74.3 / 75.4 MB (the rest of the write-back
+# is still in the 126 MB L2 when the launch ends).
+TILE_PASS_TRAFFIC = {(24, "c64"): 209.1e6}
 
 
 def _peaks():
@@ -212,13 +217,15 @@ def _config(args, p_ref, p_ours):
     }
 
 
-def batched_adjoint_leg(args, dev, steps, warmup):
+def batched_adjoint_leg(args, dev, steps, warmup, world=1, rank=0, max_over_ranks=None, barrier=None):
     """4096 uneven instances (qubits uniform 6..16, 10..40 layers of Rot on
     every wire + CX ring, independent seeded angles, <Z_0>): expectation value
     plus the full adjoint gradient of every instance in one CUDA-graph launch,
     against the plain per-circuit forward kernel driven by parameter shift
     (2 forwards per angle + 1, every shifted set of an instance in one batched
-    forward call) on a seeded sample of the instances, scaled to the workload."""
+    forward call) on a seeded sample of the instances, scaled to the workload.
+    With N ranks the instances split by estimated cost (no exchange); the
+    time is the max over ranks and the rate counts every rank's instances."""
     import torch
 
     import jaqsi_b200 as jq
@@ -240,11 +247,14 @@ def batched_adjoint_leg(args, dev, steps, warmup):
                     jq.CX(wires=[w, (w + 1) % n])
         return tape
 
+    from jaqsi_b200.shard import instance_cost, partition
+
+    mine = partition([instance_cost(n, 2 * n * d) for n, d in shapes], world)[rank]
     t0 = time.perf_counter()
-    tapes = [record(n, d, a) for (n, d), a in zip(shapes, angles)]
+    tapes = {i: record(*shapes[i], angles[i]) for i in (mine if world > 1 else range(count))}
     obs = [jq.PauliZ(0)]
     t1 = time.perf_counter()
-    bg = jq.BatchedGradients([(t, n, obs) for t, (n, _) in zip(tapes, shapes)], dtype=torch.complex64)
+    bg = jq.BatchedGradients([(tapes[i], shapes[i][0], obs) for i in mine], dtype=torch.complex64)
     print(f"[bench] batched leg: record {t1 - t0:.1f} s, build {time.perf_counter() - t1:.1f} s", file=sys.stderr,
           flush=True)
     stream = torch.cuda.current_stream()
@@ -253,14 +263,26 @@ def batched_adjoint_leg(args, dev, steps, warmup):
     torch.cuda.synchronize()
     ts = []
     for _ in range(steps):
+        if barrier:
+            barrier()
         a = torch.cuda.Event(enable_timing=True)
         b = torch.cuda.Event(enable_timing=True)
         a.record(stream)
         bg.run()
         b.record(stream)
         b.synchronize()
-        ts.append(a.elapsed_time(b))
+        t = a.elapsed_time(b)
+        ts.append(max_over_ranks(t) if max_over_ranks else t)
     ms = statistics.median(ts)
+    base = {
+        "workload": f"{count} instances, qubits uniform 6..16, 10..40 layers of Rot on every wire + CX ring, "
+                    f"<Z_0>, complex64, seeded (numpy default_rng(4))",
+        "grads_per_s": count / (ms * 1e-3), "ms_per_step": ms, "steps": steps,
+        "classes": bg.classes, "config": bg.config, "gpu_launches_per_step": "1 CUDA graph",
+        "sharding": f"cost-balanced split over {world} ranks, time = max over ranks" if world > 1 else "1 GPU",
+    }
+    if world > 1:
+        return base
     ev, grad = bg.run()
     grad64 = grad.detach().cpu().numpy().copy()
     parts = bg.split(ev.detach().cpu().numpy(), grad64)
@@ -318,10 +340,7 @@ def batched_adjoint_leg(args, dev, steps, warmup):
         del state, ws
     shift_total_ms = shift_ms * work_total / max(work_sample, 1)
     return {
-        "workload": f"{count} instances, qubits uniform 6..16, 10..40 layers of Rot on every wire + CX ring, "
-                    f"<Z_0>, complex64, seeded (numpy default_rng(4))",
-        "grads_per_s": count / (ms * 1e-3), "ms_per_step": ms, "steps": steps,
-        "classes": bg.classes, "config": bg.config,
+        **base,
         "param_shift_grads_per_s": count / (shift_total_ms * 1e-3),
         "param_shift_ms_scaled": shift_total_ms,
         "param_shift_sample": f"{len(sample)} seeded instances timed (one batched jq_forward of the 2P+1 shifted "
@@ -329,7 +348,6 @@ def batched_adjoint_leg(args, dev, steps, warmup):
         "speedup_vs_param_shift": shift_total_ms / ms,
         "max_abs_grad_err_vs_c128": max_err,
         "param_shift_max_abs_grad_err_vs_c128": ps_err,
-        "gpu_launches_per_step": "1 CUDA graph",
     }
 
 
@@ -379,6 +397,65 @@ def adjoint_20q_leg(dev, steps):
             "ms_per_grad_c64": out["c64"][0], "grads_per_s_c64": 1e3 / out["c64"][0],
             "ms_per_grad_c128": out["c128"][0], "max_abs_grad_err_c64_vs_c128": err,
             "timed": "forward + adjoint through the public API (simulate_and_measure + backward)"}
+
+
+def noisy_dm_leg(steps, batch=2):
+    """12-qubit density matrix, 20 layers of RX/RY/RZ on every wire + CX
+    ring, DepolarizingChannel(0.01) then AmplitudeDamping(0.005) on every
+    wire each gate touches, sum_i <Z_i>: forward + checkpointed reverse
+    gradient for `batch` seeded parameter sets per step through
+    Script.execute(in_axes=(0,)) and backward, complex128 and complex64."""
+    import torch
+
+    import jaqsi_b200 as jq
+
+    n, layers = 12, 20
+
+    def circuit(p):
+        for l in range(layers):
+            for w in range(n):
+                for k, gate in enumerate((jq.RX, jq.RY, jq.RZ)):
+                    gate(p[l, w, k], wires=w)
+                    jq.DepolarizingChannel(0.01, wires=w)
+                    jq.AmplitudeDamping(0.005, wires=w)
+            for w in range(n):
+                jq.CX(wires=[w, (w + 1) % n])
+                for q in (w, (w + 1) % n):
+                    jq.DepolarizingChannel(0.01, wires=q)
+                    jq.AmplitudeDamping(0.005, wires=q)
+
+    obs = [jq.PauliZ(i) for i in range(n)]
+    script = jq.Script(circuit, n_qubits=n)
+    ang = np.random.default_rng(5).uniform(0, 2 * np.pi, (batch, layers, n, 3))
+    out = {}
+    for dt, name in ((torch.complex128, "c128"), (torch.complex64, "c64")):
+        p = torch.tensor(ang, requires_grad=True)
+
+        def step():
+            p.grad = None
+            ev = script.execute("expval", obs, args=(p,), in_axes=(0,), dtype=dt)
+            ev.sum().backward()
+            return ev
+
+        step()
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(steps):
+            t0 = torch.cuda.Event(enable_timing=True)
+            t1 = torch.cuda.Event(enable_timing=True)
+            t0.record()
+            step()
+            t1.record()
+            t1.synchronize()
+            ts.append(t0.elapsed_time(t1))
+        out[name] = (statistics.median(ts), p.grad.detach().clone())
+    err = float((out["c64"][1] - out["c128"][1]).abs().max())
+    return {"workload": f"12-qubit density matrix (4096 x 4096), 20 layers RX/RY/RZ + CX ring, depolarizing 0.01 + "
+                        f"amplitude damping 0.005 after every gate, sum <Z_i>, {batch} parameter sets per step",
+            "ms_per_grad_c128": out["c128"][0] / batch, "ms_per_grad_c64": out["c64"][0] / batch,
+            "batch64_s_c128_scaled": out["c128"][0] / batch * 64e-3,
+            "max_abs_grad_err_c64_vs_c128": err,
+            "timed": "forward + checkpointed reverse through Script.execute(in_axes) and backward"}
 
 
 def ours_arm(args):
@@ -517,7 +594,10 @@ def ours_arm(args):
         "vs_baseline": None, "dtype": args.dtype, "data": "synthetic (seeded angles, |0..0>)",
         "config": _config(args, p_ref, P),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
+                     "frac": achieved / peak, "traffic": TILE_PASS_TRAFFIC.get((n, args.dtype)),
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per launch of the "
+                                       "specialised tile pass (2 launches captured, averaged)",
+                     "peak_kind": peak_kind,
                      "kernel": "jqk* (tile pass specialised per plan by NVRTC)",
                      "launches_per_step": P,
                      "avg_launch_us": sweep_ms * 1e3 / P, "bytes_per_launch": pass_bytes},
@@ -529,9 +609,11 @@ def ours_arm(args):
     }
     if not args.no_batch:
         t0 = time.perf_counter()
-        result["batched_adjoint"] = batched_adjoint_leg(args, dev, max(3, args.steps // 2), args.warmup)
+        result["batched_adjoint"] = batched_adjoint_leg(args, dev, max(3, args.steps // 2), args.warmup, world, rank,
+                                                        max_over_ranks, barrier)
         t1 = time.perf_counter()
         result["adjoint_20q"] = adjoint_20q_leg(dev, max(3, args.steps // 2))
+        result["noisy_dm_12q"] = noisy_dm_leg(2)
         print(f"[bench] batched leg {t1 - t0:.1f} s, 20-qubit adjoint leg {time.perf_counter() - t1:.1f} s",
               file=sys.stderr, flush=True)
     if rank == 0 and world == 1 and not args.no_cpu:
