@@ -234,7 +234,8 @@ def batched_adjoint_leg(args, dev, steps, warmup, world=1, rank=0, max_over_rank
 
     rng = np.random.default_rng(4)
     count = args.batch_instances
-    shapes = [(int(rng.integers(6, 17)), int(rng.integers(10, 41))) for _ in range(count)]
+    qlo, qhi = args.batch_qubits
+    shapes = [(int(rng.integers(qlo, qhi + 1)), int(rng.integers(10, 41))) for _ in range(count)]
     angles = [rng.uniform(0, 2 * np.pi, (d, n, 3)) for n, d in shapes]
 
     def record(n, d, ang):
@@ -274,15 +275,15 @@ def batched_adjoint_leg(args, dev, steps, warmup, world=1, rank=0, max_over_rank
         t = a.elapsed_time(b)
         ts.append(max_over_ranks(t) if max_over_ranks else t)
     ms = statistics.median(ts)
-    base = {
-        "workload": f"{count} instances, qubits uniform 6..16, 10..40 layers of Rot on every wire + CX ring, "
+    summary = {
+        "workload": f"{count} instances, qubits uniform {qlo}..{qhi}, 10..40 layers of Rot on every wire + CX ring, "
                     f"<Z_0>, complex64, seeded (numpy default_rng(4))",
         "grads_per_s": count / (ms * 1e-3), "ms_per_step": ms, "steps": steps,
         "classes": bg.classes, "config": bg.config, "gpu_launches_per_step": "1 CUDA graph",
         "sharding": f"cost-balanced split over {world} ranks, time = max over ranks" if world > 1 else "1 GPU",
     }
     if world > 1:
-        return base
+        return summary
     ev, grad = bg.run()
     grad64 = grad.detach().cpu().numpy().copy()
     parts = bg.split(ev.detach().cpu().numpy(), grad64)
@@ -340,7 +341,7 @@ def batched_adjoint_leg(args, dev, steps, warmup, world=1, rank=0, max_over_rank
         del state, ws
     shift_total_ms = shift_ms * work_total / max(work_sample, 1)
     return {
-        **base,
+        **summary,
         "param_shift_grads_per_s": count / (shift_total_ms * 1e-3),
         "param_shift_ms_scaled": shift_total_ms,
         "param_shift_sample": f"{len(sample)} seeded instances timed (one batched jq_forward of the 2P+1 shifted "
@@ -643,11 +644,22 @@ def main():
     ap.add_argument("--tile-bits", type=int, default=0, help="override the forward tile size (qubits per CTA)")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-adjoint and 20-qubit adjoint legs")
     ap.add_argument("--batch-instances", type=int, default=4096)
+    ap.add_argument("--batch-qubits", type=int, nargs=2, default=[6, 16], metavar=("LO", "HI"),
+                    help="qubit range of the batched instances")
+    ap.add_argument("--only-batch", action="store_true",
+                    help="run only the batched-adjoint leg on one GPU and print its JSON (profiling runs)")
     ap.add_argument("--shift-sample", type=int, default=24,
                     help="instances whose parameter-shift baseline is timed and scaled")
     args = ap.parse_args()
     if args.impl == "reference":
         return reference_arm(args)
+    if args.only_batch:
+        import torch
+
+        torch.cuda.set_device(0)
+        args.shift_sample = min(args.shift_sample, args.batch_instances)
+        print(json.dumps(batched_adjoint_leg(args, torch.device("cuda", 0), args.steps, args.warmup)))
+        return 0
     return ours_arm(args)
 
 
