@@ -224,11 +224,11 @@ def _make_rotation_gate(pauli_class, name: str, kind: int):
         _num_wires = 1
         is_unitary = True
         _param_names = ("theta",)
+        _structure = GateStructure(diagonal=pauli_class is PauliZ)
 
         def __init__(self, theta, wires: Union[int, List[int]] = 0, **kwargs) -> None:
             self.theta = theta
             super().__init__(wires=wires, **kwargs)
-            self._structure = GateStructure(diagonal=pauli_class is PauliZ)
 
         @property
         def matrix(self) -> torch.Tensor:

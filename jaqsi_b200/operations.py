@@ -16,6 +16,7 @@ import numpy as np
 import torch
 
 from jaqsi_b200 import _lib as L
+from jaqsi_b200.tape import _local as _tape_local
 from jaqsi_b200.tape import active_tape, recording  # noqa: F401  (re-export)
 
 Matrix = Union[np.ndarray, torch.Tensor]
@@ -117,21 +118,22 @@ class Operation:
         record: bool = True,
         name: Optional[str] = None,
     ) -> None:
+        # (hot: runs once per recorded op on every call of a circuit)
         self.name = name or self.__class__.__name__
-        self.wires = list(wires) if isinstance(wires, (list, tuple)) else [wires]
-        if self._num_wires is not None and len(self.wires) != self._num_wires:
-            raise ValueError(
-                f"{self.name} expects {self._num_wires} wire(s), got {len(self.wires)}: {self.wires}"
-            )
-        if len(self.wires) != len(set(self.wires)):
-            raise ValueError(f"{self.name} received duplicate wires: {self.wires}")
+        ws = list(wires) if isinstance(wires, (list, tuple)) else [wires]
+        self._wires = ws
+        nw = self._num_wires
+        if nw is not None and len(ws) != nw:
+            raise ValueError(f"{self.name} expects {nw} wire(s), got {len(ws)}: {ws}")
+        if len(ws) > 1 and len(ws) != len(set(ws)):
+            raise ValueError(f"{self.name} received duplicate wires: {ws}")
         if matrix is not None:
             self._matrix = matrix
             self._structure = GateStructure()
         if record:
-            tape = active_tape()
-            if tape is not None:
-                tape.append(self)
+            stack = getattr(_tape_local, "stack", None)
+            if stack:
+                stack[-1].append(self)
 
     # -- basic properties ----------------------------------------------------
     @property
