@@ -400,6 +400,49 @@ def adjoint_20q_leg(dev, steps):
             "timed": "forward + adjoint through the public API (simulate_and_measure + backward)"}
 
 
+def small_10q_leg(steps):
+    """10 qubits, complex128, 5 layers of RX/RY/RZ on every wire + CX ring,
+    seeded angles, <Z_i> on every wire: forward + adjoint gradient per step
+    through Script.execute and backward (a latency-bound case: 16 KiB state)."""
+    import torch
+
+    import jaqsi_b200 as jq
+
+    n, layers = 10, 5
+    ang = torch.tensor(np.random.default_rng(1).uniform(0, 2 * np.pi, (layers, n, 3)), requires_grad=True)
+
+    def circuit(a):
+        for l in range(layers):
+            for w in range(n):
+                jq.RX(a[l, w, 0], wires=w)
+                jq.RY(a[l, w, 1], wires=w)
+                jq.RZ(a[l, w, 2], wires=w)
+            for w in range(n):
+                jq.CX(wires=[w, (w + 1) % n])
+
+    script = jq.Script(circuit, n_qubits=n)
+    obs = [jq.PauliZ(i) for i in range(n)]
+
+    def step():
+        ang.grad = None
+        ev = script.execute("expval", obs, args=(ang,), dtype=torch.complex128)
+        ev.sum().backward()
+        return ev
+
+    for _ in range(3):
+        step()
+    torch.cuda.synchronize()
+    ts = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        step()
+        torch.cuda.synchronize()
+        ts.append((time.perf_counter() - t0) * 1e3)
+    return {"workload": "10 qubits c128, 5 layers RX/RY/RZ + CX ring, <Z_i> on every wire, forward + gradient",
+            "ms_per_step": statistics.median(ts),
+            "timed": "host wall clock around Script.execute + backward + synchronize (launch/host bound)"}
+
+
 def noisy_dm_leg(steps, batch=2):
     """12-qubit density matrix, 20 layers of RX/RY/RZ on every wire + CX
     ring, DepolarizingChannel(0.01) then AmplitudeDamping(0.005) on every
@@ -615,6 +658,7 @@ def ours_arm(args):
         t1 = time.perf_counter()
         result["adjoint_20q"] = adjoint_20q_leg(dev, max(3, args.steps // 2))
         result["noisy_dm_12q"] = noisy_dm_leg(2)
+        result["small_10q"] = small_10q_leg(max(5, args.steps))
         print(f"[bench] batched leg {t1 - t0:.1f} s, 20-qubit adjoint leg {time.perf_counter() - t1:.1f} s",
               file=sys.stderr, flush=True)
     if rank == 0 and world == 1 and not args.no_cpu:

@@ -261,6 +261,18 @@ JQ_API int jq_backward(const jq_plan* plan, int batch, const double* angles,
                 double* grad_angles, void* grad_mats, void* grad_init,
                 void* workspace, size_t workspace_bytes, void* stream);
 
+/* Shot sampling: `shots` basis-state draws per row from the probabilities
+ * probs float64 [batch, dim] (device; negative rounding noise counts as 0,
+ * rows need not be normalised), histogram into counts uint32 [batch, dim]
+ * (device, overwritten).  Inverse CDF over a float64 prefix sum; the
+ * random stream is a counter-based generator of (seed, row, shot), so a
+ * seed reproduces the counts exactly.  Replaces jax.random.choice + the
+ * histogram of jaqsi/simulation.py:860-917 (same distribution, not JAX's
+ * stream).  workspace: jq_sample_workspace_bytes(batch, dim) bytes. */
+JQ_API size_t jq_sample_workspace_bytes(int batch, int64_t dim);
+JQ_API int jq_sample_shots(const double* probs, int batch, int64_t dim, int64_t shots, uint64_t seed,
+                           uint32_t* counts, void* workspace, size_t workspace_bytes, void* stream);
+
 /* ------------------------------------------------------------------------
  * Batched uneven instances: forward + adjoint of many independent circuits
  * of different qubit counts, depths and parameters in one CUDA-graph launch.

@@ -51,6 +51,8 @@ EXPORTED = (
     "jq_sweep",
     "jq_adjoint",
     "jq_backward",
+    "jq_sample_workspace_bytes",
+    "jq_sample_shots",
     "jq_batch_build",
     "jq_batch_free",
     "jq_batch_info",
@@ -180,6 +182,11 @@ def _declare(lib: ctypes.CDLL) -> None:
     lib.jq_adjoint.restype = i32
     lib.jq_backward.argtypes = [vp, i32, vp, vp, vp, i32, i32, vp, vp, vp, vp, vp, vp, ctypes.c_size_t, vp]
     lib.jq_backward.restype = i32
+    lib.jq_sample_workspace_bytes.argtypes = [i32, ctypes.c_int64]
+    lib.jq_sample_workspace_bytes.restype = ctypes.c_size_t
+    lib.jq_sample_shots.argtypes = [vp, i32, ctypes.c_int64, ctypes.c_int64, ctypes.c_uint64, vp, vp,
+                                    ctypes.c_size_t, vp]
+    lib.jq_sample_shots.restype = i32
     lib.jq_batch_build.argtypes = [ctypes.POINTER(vp), i32, ctypes.POINTER(ctypes.c_int32), i32,
                                    ctypes.POINTER(JqBatchConfig), ctypes.POINTER(vp)]
     lib.jq_batch_build.restype = i32

@@ -2313,6 +2313,13 @@ int backward_impl(const jq_plan* plan, int batch, const double* angles, const vo
 
 #include "batch.cuh"
 
+size_t sample_ws_bytes(int batch, int64_t dim) {
+  const int64_t ntiles = (dim + 1023) / 1024;
+  return static_cast<size_t>(batch) * static_cast<size_t>(dim + ntiles) * sizeof(double);
+}
+
+#include "sample.cuh"
+
 jq_batch_config batch_default_config(int dtype) {
   jq_batch_config c;
   c.warp_max_qubits = dtype == JQ_C64 ? 9 : 8;
@@ -2617,6 +2624,25 @@ int jq_forward_noalloc(const jq_plan* plan, int batch, const double* angles, con
   }
   return jq_forward(plan, batch, angles, mats, init, init_batched, out_type, state, out, ws, JQ_STATIC_WS_BYTES,
                     stream);
+}
+
+// ---------------------------------------------------------------------------
+// shot sampling
+// ---------------------------------------------------------------------------
+size_t jq_sample_workspace_bytes(int batch, int64_t dim) {
+  if (batch <= 0 || dim <= 0) return 0;
+  return sample_ws_bytes(batch, dim);
+}
+
+int jq_sample_shots(const double* probs, int batch, int64_t dim, int64_t shots, uint64_t seed, uint32_t* counts,
+                    void* workspace, size_t workspace_bytes, void* stream) {
+  if (!probs || !counts || batch <= 0 || dim <= 0 || shots < 0 || dim > (int64_t(1) << 34) ||
+      shots > 0xFFFFFFFFll) {
+    set_error("jq_sample_shots: need probs and counts, batch > 0, 0 < dim <= 2^34, 0 <= shots < 2^32");
+    return JQ_EINVAL;
+  }
+  return sample_impl(probs, batch, dim, shots, seed, workspace, workspace_bytes, counts,
+                     static_cast<cudaStream_t>(stream));
 }
 
 // ---------------------------------------------------------------------------

@@ -646,20 +646,32 @@ def _generator(key, device) -> torch.Generator:
 
 
 def sample_shots(probs: torch.Tensor, n_qubits: int, type: str, obs, shots: int, key) -> torch.Tensor:
-    """Histogram of *shots* basis samples drawn from *probs* on the GPU.
+    """Histogram of *shots* basis samples drawn from *probs* on the GPU
+    (``jq_sample_shots``: inverse CDF over a float64 prefix sum).
 
-    ``key`` is an integer seed or a ``torch.Generator``; the draws are not the
+    ``key`` is an integer seed (the same seed gives the same counts) or a
+    ``torch.Generator`` (a seed is drawn from it); the draws are not the
     reference's JAX PRNG stream, only the same distribution.
     """
     if type not in ("probs", "expval"):
         raise ValueError(f"Shot simulation is only supported for 'probs' and 'expval', got {type!r}.")
     dim = 2**n_qubits
-    p = probs.detach().to(torch.float64).clamp_min(0)
-    gen = _generator(key, p.device)
-    samples = torch.multinomial(p, shots, replacement=True, generator=gen)
-    counts = torch.bincount(samples, minlength=dim).to(torch.float64)
-    est = counts / shots
+    p = probs.detach().to(torch.float64).contiguous()
+    rows = p.reshape(-1, dim)
+    if isinstance(key, torch.Generator):
+        seed = int(torch.randint(0, 2**62, (1,), generator=key, device=key.device).item())
+    else:
+        seed = 0 if key is None else int(key) & 0xFFFFFFFFFFFFFFFF
+    lib = L.lib()
+    wsb = int(lib.jq_sample_workspace_bytes(rows.shape[0], dim))
+    ws = torch.empty(max(wsb, 1), dtype=torch.uint8, device=p.device)
+    counts = torch.empty((rows.shape[0], dim), dtype=torch.int32, device=p.device)
+    L.check(lib.jq_sample_shots(_ptr(rows), rows.shape[0], dim, int(shots), seed, _ptr(counts), _ptr(ws), wsb,
+                                _stream()))
+    est = (counts.to(torch.float64) / shots).reshape(p.shape)  # shots < 2^31: int32 counts
     if type == "probs":
         return est.to(probs.dtype)
-    vals = [torch.dot(_obs_diagonal(ob, n_qubits, p.device), est) for ob in obs]
-    return torch.stack(vals).to(probs.dtype) if vals else torch.zeros(0, dtype=probs.dtype, device=p.device)
+    vals = [est @ _obs_diagonal(ob, n_qubits, p.device) for ob in obs]
+    if not vals:
+        return torch.zeros(est.shape[:-1] + (0,), dtype=probs.dtype, device=p.device)
+    return torch.stack(vals, dim=-1).to(probs.dtype)
