@@ -947,18 +947,16 @@ __global__ void __launch_bounds__(512, 1) k_tile_adj(typename CplxT<R>::T* __res
 // ---------------------------------------------------------------------------
 template <typename C, int KT>
 __device__ void bwd_dense(const C* sx, C* sl, int t, const TileOp& op, const C* __restrict__ M, double2* gacc,
-                          double* red) {
+                          double* red, double* stage = nullptr) {
   constexpr int D = 1 << KT;
   const int G = 1 << (t - op.nfix);
   const bool grad = op.grad_off >= 0;
   int off[D];
 #pragma unroll
   for (int j = 0; j < D; ++j) off[j] = target_off(j, op, KT);
-  C mh[D * D];
-#pragma unroll
-  for (int i = 0; i < D; ++i)
-#pragma unroll
-    for (int j = 0; j < D; ++j) mh[i * D + j] = cconj(M[j * D + i]);
+  // G^dagger entries are read from the (L1-cached) block matrix when used
+  // rather than held in registers: with the float64 cotangent accumulators
+  // they would not fit in a 512-thread CTA's register budget
   double2 acc[D * D];
 #pragma unroll
   for (int e = 0; e < D * D; ++e) acc[e] = make_double2(0, 0);
@@ -980,7 +978,7 @@ __device__ void bwd_dense(const C* sx, C* sl, int t, const TileOp& op, const C* 
     for (int i = 0; i < D; ++i) {
       C a = cmake<C>(0, 0);
 #pragma unroll
-      for (int j = 0; j < D; ++j) a = cfma(mh[i * D + j], vl[j], a);
+      for (int j = 0; j < D; ++j) a = cfma(cconj(__ldg(&M[j * D + i])), vl[j], a);
       sl[base + off[i]] = a;
     }
   }
@@ -992,7 +990,10 @@ __device__ void bwd_dense(const C* sx, C* sl, int t, const TileOp& op, const C* 
       vals[2 * e + 1] = acc[e].y;
     }
     block_reduce<2 * D * D>(vals, red);
-    if (threadIdx.x < 2 * D * D) atomicAdd(reinterpret_cast<double*>(gacc + op.grad_off) + threadIdx.x, vals[0]);
+    if (threadIdx.x < 2 * D * D) {
+      if (stage) stage[threadIdx.x] += vals[0];  // per-CTA staging, flushed by the caller
+      else atomicAdd(reinterpret_cast<double*>(gacc + op.grad_off) + threadIdx.x, vals[0]);
+    }
   }
 }
 
@@ -1032,7 +1033,7 @@ __device__ __noinline__ void bwd_dense_wide(const C* sx, C* sl, int t, const Til
 
 template <typename C>
 __device__ void bwd_diag(const C* sx, C* sl, int t, const TileOp& op, const C* __restrict__ Dg, double2* gacc,
-                         double* red) {
+                         double* red, double* stage = nullptr) {
   const int kt = op.kt, D = 1 << kt;
   const int G = 1 << (t - op.nfix);
   const bool grad = op.grad_off >= 0;
@@ -1062,7 +1063,10 @@ __device__ void bwd_diag(const C* sx, C* sl, int t, const TileOp& op, const C* _
       vals[2 * q + 1] = acc[q].y;
     }
     block_reduce<8>(vals, red);
-    if (threadIdx.x < 2 * D) atomicAdd(reinterpret_cast<double*>(gacc + op.grad_off) + threadIdx.x, vals[0]);
+    if (threadIdx.x < 2 * D) {
+      if (stage) stage[threadIdx.x] += vals[0];
+      else atomicAdd(reinterpret_cast<double*>(gacc + op.grad_off) + threadIdx.x, vals[0]);
+    }
   }
 }
 
@@ -1079,7 +1083,32 @@ __global__ void __launch_bounds__(512, 1) k_tile_bwd(const typename CplxT<R>::T*
   C* sl = sx + (1 << t);
   double* red = reinterpret_cast<double*>(sl + (1 << t));
   uint32_t* tbl = reinterpret_cast<uint32_t*>(red + 32 * kRedSlots);
+  // cotangent partial sums of this CTA's tiles (32 doubles per op of the
+  // pass), added to the instance's accumulators once per instance instead
+  // of one set of same-address global atomics per tile
+  double* stage = reinterpret_cast<double*>(tbl + (((1 << (t - c)) + 1) & ~1));
+  const int nops = pd.op_end - pd.op_begin;
+  for (int e = threadIdx.x; e < 32 * nops; e += blockDim.x) stage[e] = 0.0;
   fill_table(tbl, pd);
+  auto stage_slot = [&](const TileOp& op) -> bool {
+    // register-reduced forms only; wide blocks keep direct atomics
+    return (op.kind == BK_DENSE && op.kt <= 2) || (op.kind == BK_DIAG && op.kt <= 2);
+  };
+  auto flush = [&](int64_t inst) {
+    __syncthreads();
+    double* g = reinterpret_cast<double*>(gacc + inst * grad_stride);
+    for (int k = 0; k < nops; ++k) {
+      const TileOp& op = ops[pd.op_begin + k];
+      if (op.grad_off < 0 || !stage_slot(op)) continue;
+      const int nv = op.kind == BK_DENSE ? 2 * (1 << op.kt) * (1 << op.kt) : 2 * (1 << op.kt);
+      for (int e = threadIdx.x; e < nv; e += blockDim.x) {
+        atomicAdd(g + 2 * op.grad_off + e, stage[32 * k + e]);
+        stage[32 * k + e] = 0.0;
+      }
+    }
+    __syncthreads();
+  };
+  int64_t last_inst = -1;
   const int64_t tiles_per = 1LL << (nb - t);
   const int64_t ntiles = tiles_per * batch;
   const uint64_t full = (nb >= 64) ? ~0ULL : ((1ULL << nb) - 1);
@@ -1090,6 +1119,10 @@ __global__ void __launch_bounds__(512, 1) k_tile_bwd(const typename CplxT<R>::T*
     const uint64_t o = (inst << nb) + pdep64(ti, outer_mask);
     const C* bm = bmat + inst * bmat_stride;
     double2* ga = gacc ? gacc + inst * grad_stride : nullptr;
+    if (gacc && inst != last_inst) {
+      if (last_inst >= 0) flush(last_inst);
+      last_inst = inst;
+    }
     __syncthreads();
     tile_load(sx, x + o, tbl, t, c);
     tile_load(sl, lam + o, tbl, t, c);
@@ -1100,18 +1133,21 @@ __global__ void __launch_bounds__(512, 1) k_tile_bwd(const typename CplxT<R>::T*
       switch (op.kind) {
         case BK_DENSE:
           switch (op.kt) {
-            case 1: bwd_dense<C, 1>(sx, sl, t, op, bm + op.mat_off, ga, red); break;
-            case 2: bwd_dense<C, 2>(sx, sl, t, op, bm + op.mat_off, ga, red); break;
+            case 1: bwd_dense<C, 1>(sx, sl, t, op, bm + op.mat_off, ga, red, stage + 32 * (oi - pd.op_begin)); break;
+            case 2: bwd_dense<C, 2>(sx, sl, t, op, bm + op.mat_off, ga, red, stage + 32 * (oi - pd.op_begin)); break;
             default: bwd_dense_wide<C>(sx, sl, t, op, bm + op.mat_off, ga); break;
           }
           break;
-        case BK_DIAG: bwd_diag<C>(sx, sl, t, op, bm + op.mat_off, ga, red); break;
+        case BK_DIAG:
+          bwd_diag<C>(sx, sl, t, op, bm + op.mat_off, ga, red, op.kt <= 2 ? stage + 32 * (oi - pd.op_begin) : nullptr);
+          break;
         default: tile_apply<C>(sl, t, op, bm, perms, true); break;
       }
       __syncthreads();
     }
     tile_store(sl, lam + o, tbl, t, c);
   }
+  if (gacc && last_inst >= 0) flush(last_inst);
 }
 
 // ---------------------------------------------------------------------------
@@ -2283,7 +2319,7 @@ int backward_impl(const jq_plan* plan, int batch, const double* angles, const vo
     for (int64_t p = p1 - 1; p >= p0; --p) {
       const PassDesc& pd = sch.passes[p];
       if (pd.op_end == pd.op_begin) continue;
-      const size_t smem = tile_smem<R>(pd, 2);
+      const size_t smem = tile_smem<R>(pd, 2) + 8 + 32 * sizeof(double) * static_cast<size_t>(pd.op_end - pd.op_begin);
       const int64_t ntiles = (1LL << (plan->n_bits - pd.t)) * batch;
       const int ctas = ctas_for(k_tile_bwd<R>, plan->threads, smem, ntiles);
       k_tile_bwd<R><<<ctas, plan->threads, smem, st>>>(seg(p - p0), lam, plan->n_bits, batch, pd, T->bwd_ops, bmat,
