@@ -1086,8 +1086,11 @@ __global__ void __launch_bounds__(512, 1) k_tile_bwd(const typename CplxT<R>::T*
   // cotangent partial sums of this CTA's tiles (32 doubles per op of the
   // pass), added to the instance's accumulators once per instance instead
   // of one set of same-address global atomics per tile
-  double* stage = reinterpret_cast<double*>(tbl + (((1 << (t - c)) + 1) & ~1));
+  double* stage = reinterpret_cast<double*>(tbl + (((1 << (t - c)) + 3) & ~3));
   const int nops = pd.op_end - pd.op_begin;
+  // passes of several blocks: the state before block j is recomputed in a
+  // third tile from the state before the pass (blocks op_begin..j-1)
+  C* sw = reinterpret_cast<C*>(stage + 32 * nops);
   for (int e = threadIdx.x; e < 32 * nops; e += blockDim.x) stage[e] = 0.0;
   fill_table(tbl, pd);
   auto stage_slot = [&](const TileOp& op) -> bool {
@@ -1128,18 +1131,28 @@ __global__ void __launch_bounds__(512, 1) k_tile_bwd(const typename CplxT<R>::T*
     tile_load(sl, lam + o, tbl, t, c);
     __syncthreads();
     for (int oi = pd.op_end - 1; oi >= pd.op_begin; --oi) {
+      C* xs = sx;
+      if (oi > pd.op_begin) {
+        for (int e = threadIdx.x; e < (1 << t); e += blockDim.x) sw[e] = sx[e];
+        __syncthreads();
+        for (int k = pd.op_begin; k < oi; ++k) {
+          tile_apply<C>(sw, t, ops[k], bm, perms, false);
+          __syncthreads();
+        }
+        xs = sw;
+      }
       TileOp op = ops[oi];
       if (!ga) op.grad_off = -1;
       switch (op.kind) {
         case BK_DENSE:
           switch (op.kt) {
-            case 1: bwd_dense<C, 1>(sx, sl, t, op, bm + op.mat_off, ga, red, stage + 32 * (oi - pd.op_begin)); break;
-            case 2: bwd_dense<C, 2>(sx, sl, t, op, bm + op.mat_off, ga, red, stage + 32 * (oi - pd.op_begin)); break;
-            default: bwd_dense_wide<C>(sx, sl, t, op, bm + op.mat_off, ga); break;
+            case 1: bwd_dense<C, 1>(xs, sl, t, op, bm + op.mat_off, ga, red, stage + 32 * (oi - pd.op_begin)); break;
+            case 2: bwd_dense<C, 2>(xs, sl, t, op, bm + op.mat_off, ga, red, stage + 32 * (oi - pd.op_begin)); break;
+            default: bwd_dense_wide<C>(xs, sl, t, op, bm + op.mat_off, ga); break;
           }
           break;
         case BK_DIAG:
-          bwd_diag<C>(sx, sl, t, op, bm + op.mat_off, ga, red, op.kt <= 2 ? stage + 32 * (oi - pd.op_begin) : nullptr);
+          bwd_diag<C>(xs, sl, t, op, bm + op.mat_off, ga, red, op.kt <= 2 ? stage + 32 * (oi - pd.op_begin) : nullptr);
           break;
         default: tile_apply<C>(sl, t, op, bm, perms, true); break;
       }
@@ -1901,7 +1914,7 @@ WsLayout layout(const jq_plan* plan, int batch, int mode_grad /*0 fwd, 1 adjoint
     off += align256(state);
   }
   if (mode_grad == 2) {
-    const int64_t P = static_cast<int64_t>(plan->bwd.passes.size());
+    const int64_t P = static_cast<int64_t>(plan->fwd.passes.size());
     int64_t S = plan->ckpt_stride > 0 ? plan->ckpt_stride : static_cast<int64_t>(std::ceil(std::sqrt(static_cast<double>(std::max<int64_t>(P, 1)))));
     S = std::max<int64_t>(1, S);
     L.seg_len = S;
@@ -2295,12 +2308,18 @@ int backward_impl(const jq_plan* plan, int batch, const double* angles, const vo
   k_init<R><<<grid_for(elems * batch, 256), 256, 0, st>>>(work, elems, batch, static_cast<const C*>(init), dim,
                                                           init_batched, dm && init ? 1 : 0);
   JQ_CUDA(cudaGetLastError());
-  const Schedule& sch = plan->bwd;
+  // The reverse walks the fused forward schedule: checkpoints every S passes,
+  // recompute of a segment with the (specialised) forward passes, and one
+  // k_tile_bwd per pass that recomputes the states between the pass's
+  // blocks inside each tile.
+  const Schedule& sch = plan->fwd;
+  const TileOp* sops = T->fwd_ops;
+  const JitModule* jm = static_cast<const JitModule*>(T->jit);
   const int64_t P = static_cast<int64_t>(sch.passes.size());
   const int64_t S = L.seg_len;
   for (int64_t p = 0; p < P; ++p) {
     if (p % S == 0) JQ_CUDA(cudaMemcpyAsync(ckpt(p / S), work, sizeof(C) * elems * batch, cudaMemcpyDeviceToDevice, st));
-    if ((rc = run_passes<R>(plan, sch, T->bwd_ops, T->bwd_steps, T->bwd_rops, T, work, batch, bmat, p, p + 1, st))) return rc;
+    if ((rc = run_passes<R>(plan, sch, sops, T->fwd_steps, T->fwd_rops, T, work, batch, bmat, p, p + 1, st, jm))) return rc;
   }
   // seed
   if (dm) rc = seed_dm<R>(plan, T, batch, out_type, ct, ct_state, lam, st);
@@ -2314,15 +2333,17 @@ int backward_impl(const jq_plan* plan, int batch, const double* angles, const vo
     JQ_CUDA(cudaMemcpyAsync(seg(0), ckpt(c), sizeof(C) * elems * batch, cudaMemcpyDeviceToDevice, st));
     for (int64_t j = 0; j + 1 < p1 - p0; ++j) {
       JQ_CUDA(cudaMemcpyAsync(seg(j + 1), seg(j), sizeof(C) * elems * batch, cudaMemcpyDeviceToDevice, st));
-      if ((rc = run_passes<R>(plan, sch, T->bwd_ops, T->bwd_steps, T->bwd_rops, T, seg(j + 1), batch, bmat, p0 + j, p0 + j + 1, st))) return rc;
+      if ((rc = run_passes<R>(plan, sch, sops, T->fwd_steps, T->fwd_rops, T, seg(j + 1), batch, bmat, p0 + j, p0 + j + 1, st, jm))) return rc;
     }
     for (int64_t p = p1 - 1; p >= p0; --p) {
       const PassDesc& pd = sch.passes[p];
       if (pd.op_end == pd.op_begin) continue;
-      const size_t smem = tile_smem<R>(pd, 2) + 8 + 32 * sizeof(double) * static_cast<size_t>(pd.op_end - pd.op_begin);
+      const int nops = pd.op_end - pd.op_begin;
+      const size_t smem = tile_smem<R>(pd, 2) + 16 + 32 * sizeof(double) * static_cast<size_t>(nops) +
+                          (nops > 1 ? (static_cast<size_t>(1) << pd.t) * sizeof(C) : 0);
       const int64_t ntiles = (1LL << (plan->n_bits - pd.t)) * batch;
       const int ctas = ctas_for(k_tile_bwd<R>, plan->threads, smem, ntiles);
-      k_tile_bwd<R><<<ctas, plan->threads, smem, st>>>(seg(p - p0), lam, plan->n_bits, batch, pd, T->bwd_ops, bmat,
+      k_tile_bwd<R><<<ctas, plan->threads, smem, st>>>(seg(p - p0), lam, plan->n_bits, batch, pd, sops, bmat,
                                                         plan->bmat_stride, T->perm_pool, want_grad ? gacc : nullptr,
                                                         plan->grad_stride);
     }
