@@ -334,6 +334,8 @@ void emit_pass(std::ostringstream& o, const jq_plan* plan, const Schedule& s, in
   // complex128 needs about 168
   int minb = std::max(1, std::min(8, 65536 / (nthr * (c64 ? 128 : 168))));
   if (const char* e = std::getenv("JQ_JIT_MINB")) minb = std::max(1, std::min(16, std::atoi(e)));
+  // complex64 dense blocks use packed two-lane FMA unless JQ_JIT_SCALAR=1
+  const bool packed = c64 && !(std::getenv("JQ_JIT_SCALAR") && std::atoi(std::getenv("JQ_JIT_SCALAR")) == 1);
   const uint64_t full = (nb >= 64) ? ~0ULL : ((1ULL << nb) - 1);
   const uint64_t outer = full & ~pd.tile_mask;
   const int smat_pad = (pd.smat_len + 1) & ~1;
@@ -424,7 +426,7 @@ void emit_pass(std::ostringstream& o, const jq_plan* plan, const Schedule& s, in
       if (guard) o << "      if ((tid & " << ctm << "u) == " << ctm << "u) {\n";
       else o << "      {\n";
       auto V = [&](int j) { return std::string("v") + std::to_string(var[j]); };
-      if (kind == RK_DENSE1 && c64) {
+      if (kind == RK_DENSE1 && packed) {
         o << "        const float4* mq = (const float4*)smatb + " << M << ";\n";
         o << "        const float4 A = mq[0], Bq = mq[1], Cq = mq[2], Dq = mq[3];\n";
         o << "        const float2 ar = lo2(A), ai = hi2(A), br = lo2(Bq), bi = hi2(Bq), cr = lo2(Cq), ci = hi2(Cq), "
@@ -465,7 +467,7 @@ void emit_pass(std::ostringstream& o, const jq_plan* plan, const Schedule& s, in
           for (uint32_t i = 0; i < dk; ++i) idx = (idx << 1) | ((j >> ((dq >> (3 * i)) & 7u)) & 1);
           o << "        " << V(j) << " = cmul(smat[" << M + idx << "], " << V(j) << ");\n";
         }
-      } else if (kind == RK_DENSE2 && c64) {
+      } else if (kind == RK_DENSE2 && packed) {
         for (int j = 0; j < nr; ++j) {
           if (((j >> q1) & 1) || ((j >> q2) & 1)) continue;
           if ((static_cast<uint32_t>(j) & crm) != crm) continue;

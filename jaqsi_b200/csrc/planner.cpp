@@ -244,7 +244,7 @@ void build_steps(Schedule& s, const std::vector<int32_t>& perm_pool, int dtype) 
   // register bits per stage (amplitudes per thread = 2^r); JQ_REG_BITS=3
   // selects 8 amplitudes per thread (more threads, more stages)
   int r = 4;
-  if (const char* e = std::getenv("JQ_REG_BITS")) r = (std::atoi(e) == 3) ? 3 : 4;
+  if (const char* e = std::getenv("JQ_REG_BITS")) r = std::max(3, std::min(5, std::atoi(e)));
   s.reg_bits = r;
   for (PassDesc& pd : s.passes) {
     pd.step_begin = pd.step_end = static_cast<int32_t>(s.steps.size());
