@@ -181,10 +181,21 @@ class Operation:
             raise NotImplementedError(f"{self.__class__.__name__} does not define a matrix.")
         if isinstance(m, torch.Tensor):
             return L.JQ_K_MATRIX, [], m
+        cls = self.__class__
+        if m is cls._matrix:
+            # class-constant matrix: converted once per class
+            c = cls.__dict__.get("_jq_const")
+            if c is None:
+                c = np.asarray(m, dtype=np.complex128)
+                cls._jq_const = c
+            return L.JQ_K_CONST, [], c
         return L.JQ_K_CONST, [], np.asarray(m, dtype=np.complex128)
 
     def _jq_static_key(self):
         """Hashable part of the lowering that selects the execution plan."""
+        cls = self.__class__
+        if cls._matrix is not None and self._matrix is cls._matrix and not isinstance(self._matrix, torch.Tensor):
+            return (cls.__name__,)
         kind, _, payload = self._jq_lower()
         if kind == L.JQ_K_CONST:
             if self.__class__._matrix is not None and self._matrix is self.__class__._matrix:

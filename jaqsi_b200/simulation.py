@@ -191,15 +191,19 @@ def lower_tape(tape: Sequence[Operation], n_qubits: int) -> Lowered:
     keys = []
     n_ang = 0
     n_mat = 0
+    max_wires = L.JQ_MAX_OP_WIRES
+    k_matrix, k_paulirot = L.JQ_K_MATRIX, L.JQ_K_PAULIROT
+    tensor = torch.Tensor
+    angles_out = lw.angles
     for op in tape:
         if isinstance(op, Barrier):
             continue
-        wires = tuple(op.wires)
-        for w in wires:
-            if w < 0 or w >= n_qubits:
-                raise ValueError(f"{op.name}: wire {w} outside 0..{n_qubits - 1}")
-        if len(wires) > L.JQ_MAX_OP_WIRES:
-            raise ValueError(f"{op.name}: gates on more than {L.JQ_MAX_OP_WIRES} wires are not supported")
+        wires = tuple(op._wires)
+        if wires and (min(wires) < 0 or max(wires) >= n_qubits):
+            bad = [w for w in wires if w < 0 or w >= n_qubits][0]
+            raise ValueError(f"{op.name}: wire {bad} outside 0..{n_qubits - 1}")
+        if len(wires) > max_wires:
+            raise ValueError(f"{op.name}: gates on more than {max_wires} wires are not supported")
         kind, angles, payload = op._jq_lower()
         st = op._structure
         unitary = bool(op.is_unitary)
@@ -210,9 +214,12 @@ def lower_tape(tape: Sequence[Operation], n_qubits: int) -> Lowered:
         if angles:
             angle_slot = n_ang
             n_ang += len(angles)
-            lw.angles.extend(angles)
-            grad = int(any(_is_tensor(a) for a in angles))
-        if kind == L.JQ_K_MATRIX:
+            angles_out.extend(angles)
+            for a in angles:
+                if isinstance(a, tensor):
+                    grad = 1
+                    break
+        if kind == k_matrix:
             mat_slot = n_mat
             t = payload
             mat_is_diag = int(t.dim() == 1)
@@ -222,7 +229,7 @@ def lower_tape(tape: Sequence[Operation], n_qubits: int) -> Lowered:
         skey = op._jq_static_key()
         px = getattr(op, "_px", 0)
         pz = getattr(op, "_pz", 0)
-        nctrl = getattr(op, "n_controls", 0) if kind == L.JQ_K_PAULIROT else st.controls
+        nctrl = getattr(op, "n_controls", 0) if kind == k_paulirot else st.controls
         keys.append((skey, wires, st, grad, unitary, mat_is_diag))
         lw.statics.append((kind, wires, st, angle_slot, mat_slot, mat_is_diag, px, pz, nctrl, payload, grad, unitary))
         if not unitary:
