@@ -25,6 +25,9 @@ struct BBlock {
   int32_t perm;      // BK_PERM: output row r takes input row (perm >> 2r) & 3
   int32_t grad_off;  // complex128 offset of the block cotangent, -1 if none
   int32_t mat_off;   // run-dtype complex offset of the inner matrix / diagonal
+  int32_t pair;      // 1: this block and the next are uncontrolled one-target dense
+                     // blocks on different bits, applied in one sweep (greedy,
+                     // non-overlapping, so the reverse walk finds the same pairs)
 };
 
 struct BPlan {
@@ -210,6 +213,101 @@ __device__ void bapply(C* s, int n, const BBlock& B, const C* bm, int lt, int gs
   }
 }
 
+// Two uncontrolled one-target dense blocks A (bit qa) then B (bit qb) in one
+// sweep: each thread takes groups of 4 amplitudes {i, i|b, i|a, i|a|b}.
+template <typename C>
+__device__ void bapply2(C* s, int n, const BBlock& A, const BBlock& B, const C* bm, int lt, int gs) {
+  const int dim = 1 << n, qa = A.tb0, qb = B.tb0;
+  const int lo = min(qa, qb), hi = max(qa, qb);
+  const C* MA = bm + A.mat_off;
+  const C* MB = bm + B.mat_off;
+  const C a0 = MA[0], a1 = MA[1], a2 = MA[2], a3 = MA[3];
+  const C b0 = MB[0], b1 = MB[1], b2 = MB[2], b3 = MB[3];
+  for (int g = lt; g < (dim >> 2); g += gs) {
+    const int i = ins0(ins0(g, lo), hi);
+    const int ia = i | (1 << qa), ib = i | (1 << qb), iab = ia | (1 << qb);
+    C x00 = s[i], x01 = s[ib], x10 = s[ia], x11 = s[iab];
+    // A on qa: pairs (x00, x10), (x01, x11)
+    C y00 = cfma(a1, x10, cmul(a0, x00)), y10 = cfma(a3, x10, cmul(a2, x00));
+    C y01 = cfma(a1, x11, cmul(a0, x01)), y11 = cfma(a3, x11, cmul(a2, x01));
+    // B on qb: pairs (y00, y01), (y10, y11)
+    s[i] = cfma(b1, y01, cmul(b0, y00));
+    s[ib] = cfma(b3, y01, cmul(b2, y00));
+    s[ia] = cfma(b1, y11, cmul(b0, y10));
+    s[iab] = cfma(b3, y11, cmul(b2, y10));
+  }
+}
+
+// Reverse of bapply2: un-apply B then A, each with its cotangent.
+template <typename C, bool WARP>
+__device__ void badjoint2(C* sp, C* sl, int n, const BBlock& A, const BBlock& B, const C* bm, double* ga, int lt,
+                          int gs) {
+  using Acc = typename AccT<C>::T;
+  const int dim = 1 << n, qa = A.tb0, qb = B.tb0;
+  const int lo = min(qa, qb), hi = max(qa, qb);
+  const C* MA = bm + A.mat_off;
+  const C* MB = bm + B.mat_off;
+  // G^dagger = [[conj m00, conj m10], [conj m01, conj m11]]
+  const C ha00 = cconj(MA[0]), ha01 = cconj(MA[2]), ha10 = cconj(MA[1]), ha11 = cconj(MA[3]);
+  const C hb00 = cconj(MB[0]), hb01 = cconj(MB[2]), hb10 = cconj(MB[1]), hb11 = cconj(MB[3]);
+  const bool gA = ga && A.grad_off >= 0, gB = ga && B.grad_off >= 0;
+  Acc g[16];
+#pragma unroll
+  for (int e = 0; e < 16; ++e) g[e] = Acc(0);
+  for (int gi = lt; gi < (dim >> 2); gi += gs) {
+    const int i = ins0(ins0(gi, lo), hi);
+    const int ia = i | (1 << qa), ib = i | (1 << qb), iab = ia | (1 << qb);
+    C p00 = sp[i], p01 = sp[ib], p10 = sp[ia], p11 = sp[iab];
+    C l00 = sl[i], l01 = sl[ib], l10 = sl[ia], l11 = sl[iab];
+    // un-apply B on qb: pairs (00, 01), (10, 11)
+    {
+      const C q00 = cfma(hb01, p01, cmul(hb00, p00)), q01 = cfma(hb11, p01, cmul(hb10, p00));
+      const C q10 = cfma(hb01, p11, cmul(hb00, p10)), q11 = cfma(hb11, p11, cmul(hb10, p10));
+      acc_lconjp(g[8], g[9], l00, q00);
+      acc_lconjp(g[10], g[11], l00, q01);
+      acc_lconjp(g[12], g[13], l01, q00);
+      acc_lconjp(g[14], g[15], l01, q01);
+      acc_lconjp(g[8], g[9], l10, q10);
+      acc_lconjp(g[10], g[11], l10, q11);
+      acc_lconjp(g[12], g[13], l11, q10);
+      acc_lconjp(g[14], g[15], l11, q11);
+      const C m00 = cfma(hb01, l01, cmul(hb00, l00)), m01 = cfma(hb11, l01, cmul(hb10, l00));
+      const C m10 = cfma(hb01, l11, cmul(hb00, l10)), m11 = cfma(hb11, l11, cmul(hb10, l10));
+      p00 = q00; p01 = q01; p10 = q10; p11 = q11;
+      l00 = m00; l01 = m01; l10 = m10; l11 = m11;
+    }
+    // un-apply A on qa: pairs (00, 10), (01, 11)
+    {
+      const C q00 = cfma(ha01, p10, cmul(ha00, p00)), q10 = cfma(ha11, p10, cmul(ha10, p00));
+      const C q01 = cfma(ha01, p11, cmul(ha00, p01)), q11 = cfma(ha11, p11, cmul(ha10, p01));
+      acc_lconjp(g[0], g[1], l00, q00);
+      acc_lconjp(g[2], g[3], l00, q10);
+      acc_lconjp(g[4], g[5], l10, q00);
+      acc_lconjp(g[6], g[7], l10, q10);
+      acc_lconjp(g[0], g[1], l01, q01);
+      acc_lconjp(g[2], g[3], l01, q11);
+      acc_lconjp(g[4], g[5], l11, q01);
+      acc_lconjp(g[6], g[7], l11, q11);
+      sp[i] = q00; sp[ib] = q01; sp[ia] = q10; sp[iab] = q11;
+      sl[i] = cfma(ha01, l10, cmul(ha00, l00));
+      sl[ia] = cfma(ha11, l10, cmul(ha10, l00));
+      sl[ib] = cfma(ha01, l11, cmul(ha00, l01));
+      sl[iab] = cfma(ha11, l11, cmul(ha10, l01));
+    }
+  }
+  // g[0..7]: A's cotangent, g[8..15]: B's (every lane takes part in both reductions)
+  Acc gav[8], gbv[8];
+#pragma unroll
+  for (int e = 0; e < 8; ++e) {
+    gav[e] = g[e];
+    gbv[e] = g[8 + e];
+  }
+  if (ga && (A.grad_off >= 0 || B.grad_off >= 0)) {
+    if (gA) gacc_add_acc<WARP, 8>(gav, ga + 2 * A.grad_off);
+    if (gB) gacc_add_acc<WARP, 8>(gbv, ga + 2 * B.grad_off);
+  }
+}
+
 // Adjoint of one block: psi <- G^dagger psi, cotangent += lam psi^dagger
 // (psi after the un-apply), lam <- G^dagger lam.
 template <typename C, bool WARP>
@@ -355,8 +453,14 @@ __global__ void __launch_bounds__(512, 1) k_batch(BatchArgs a) {
     for (int e = lt; e < P.grad_stride; e += gs) gacc[e] = make_double2(0.0, 0.0);
     for (int j = lt; j < dim; j += gs) sp[j] = cmake<C>(j == 0 ? 1.0 : 0.0, 0.0);
     gsync<WARP>();
-    for (int b = 0; b < P.nblocks; ++b) {
-      bapply<C>(sp, n, BB[b], bm, lt, gs);
+    for (int b = 0; b < P.nblocks;) {
+      if (BB[b].pair) {
+        bapply2<C>(sp, n, BB[b], BB[b + 1], bm, lt, gs);
+        b += 2;
+      } else {
+        bapply<C>(sp, n, BB[b], bm, lt, gs);
+        b += 1;
+      }
       gsync<WARP>();
     }
     // expectation values; lambda = 2 sum_o ct_o coeff_o P_o psi
@@ -378,8 +482,14 @@ __global__ void __launch_bounds__(512, 1) k_batch(BatchArgs a) {
       if (lt == 0) a.expval[I.out_off + o] = ob.coeff * tot;
     }
     gsync<WARP>();
-    for (int b = P.nblocks - 1; b >= 0; --b) {
-      badjoint<C, WARP>(sp, sl, n, BB[b], bm, reinterpret_cast<double*>(gacc), lt, gs);
+    for (int b = P.nblocks - 1; b >= 0;) {
+      if (b >= 1 && BB[b - 1].pair) {
+        badjoint2<C, WARP>(sp, sl, n, BB[b - 1], BB[b], bm, reinterpret_cast<double*>(gacc), lt, gs);
+        b -= 2;
+      } else {
+        badjoint<C, WARP>(sp, sl, n, BB[b], bm, reinterpret_cast<double*>(gacc), lt, gs);
+        b -= 1;
+      }
       gsync<WARP>();
     }
     for (int b = lt; b < P.nblocks; b += gs)
@@ -650,6 +760,12 @@ __global__ void __launch_bounds__(512, 1) k_batch_cluster(ClusterArgs ca) {
     // forward
     for (int b = 0; b < P.nblocks; ++b) {
       const BBlock B = BB[b];
+      if (B.pair && B.tb0 < lb && BB[b + 1].tb0 < lb) {
+        bapply2<C>(sp, lb, B, BB[b + 1], bm, lt, gs);
+        __syncthreads();
+        ++b;
+        continue;
+      }
       if (!bdist(B, lb)) {
         bapply<C>(sp, lb, B, bm, lt, gs, gbase);
         __syncthreads();
@@ -739,6 +855,12 @@ __global__ void __launch_bounds__(512, 1) k_batch_cluster(ClusterArgs ca) {
     // adjoint
     for (int b = P.nblocks - 1; b >= 0; --b) {
       const BBlock B = BB[b];
+      if (b >= 1 && BB[b - 1].pair && BB[b - 1].tb0 < lb && B.tb0 < lb) {
+        badjoint2<C, false>(sp, sl, lb, BB[b - 1], B, bm, reinterpret_cast<double*>(gacc), lt, gs);
+        __syncthreads();
+        --b;
+        continue;
+      }
       if (!bdist(B, lb)) {
         badjoint<C, false>(sp, sl, lb, B, bm, reinterpret_cast<double*>(gacc), lt, gs, gbase);
         __syncthreads();

@@ -2764,6 +2764,17 @@ int jq_batch_build(jq_plan* const* plans, int n_plans, const int32_t* plan_of, i
     }
     for (const DevOp& o : pl->ops) b->ops.push_back(o);
     b->cpool.insert(b->cpool.end(), pl->const_pool.begin(), pl->const_pool.end());
+    // pair consecutive uncontrolled one-target dense blocks on different bits
+    // (greedy from the front; a paired block is never the first of another pair)
+    for (int i = 0; i + 1 < bp.nblocks; ++i) {
+      BBlock& x = b->bblk[bp.blk_off + i];
+      const BBlock& y = b->bblk[bp.blk_off + i + 1];
+      auto single = [](const BBlock& q) { return q.kind == BK_DENSE && q.nt == 1 && q.cmask == 0; };
+      if (single(x) && single(y) && x.tb0 != y.tb0) {
+        x.pair = 1;
+        ++i;
+      }
+    }
     for (const DevObs& o : pl->obs) b->obs.push_back(o);
     b->bplans.push_back(bp);
   }
