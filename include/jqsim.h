@@ -166,7 +166,8 @@ JQ_API int jq_plan_free(jq_plan* plan);
 JQ_API int jq_plan_get_info(const jq_plan* plan, jq_plan_info* info);
 
 /* Schedule of a plan: pass index of every fused block (which = 0 forward,
- * 1 adjoint, 2 checkpointed reverse) into block_pass[0..n-1], and the wires
+ * also walked backwards by jq_backward; 1 adjoint interpreter; 2 one block
+ * per pass, the unfused order) into block_pass[0..n-1], and the wires
  * of each block into block_wires[6 * b ..] (-1 padded) when non-NULL.
  * Diagnostic; no reference counterpart (the reference runs one pass per
  * entry of its plan, jaqsi/simulation.py:400-409). */

@@ -180,7 +180,7 @@ struct jq_plan {
   std::vector<int32_t> perm_pool;
   std::vector<jq::DevObs> obs;
   std::vector<double> obs_pool;
-  jq::Schedule fwd, adj, bwd;  // bwd: one block per pass (checkpointed reverse)
+  jq::Schedule fwd, adj, bwd;  // bwd: one block per pass (the unfused order; diagnostics)
   int64_t bmat_stride = 0;     // run-dtype complex elements per instance
   int64_t grad_stride = 0;     // complex128 elements per instance
   int64_t scratch_stride = 0;  // complex128 elements per instance (k > 2 blocks)
