@@ -70,29 +70,68 @@ def _records(ang):
 
 
 class Clocks:
-    """nvidia-smi samples of the SM clock and throttle reasons while timing."""
+    """SM clock and throttle-reason samples while timing: NVML read-only
+    queries every 10 ms (pynvml), else nvidia-smi every 200 ms."""
+
+    _NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
 
     def __init__(self, index: int):
         self.index = index
-        self.rows = []
+        self.rows = []  # (sm_mhz, sm_max_mhz, {reason: active})
+        self.source = None
         self._stop = threading.Event()
         self._t = None
 
+    def _nvml_sampler(self):
+        try:
+            import pynvml
+
+            pynvml.nvmlInit()
+            h = pynvml.nvmlDeviceGetHandleByIndex(self.index)
+            mx = pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM)
+            bits = (pynvml.nvmlClocksEventReasonHwSlowdown, pynvml.nvmlClocksEventReasonHwThermalSlowdown,
+                    pynvml.nvmlClocksEventReasonSwThermalSlowdown, pynvml.nvmlClocksEventReasonSwPowerCap)
+        except Exception:
+            return None
+
+        def sample():
+            sm = pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)
+            r = pynvml.nvmlDeviceGetCurrentClocksEventReasons(h)
+            return float(sm), float(mx), {n: bool(r & b) for n, b in zip(self._NAMES, bits)}
+
+        try:
+            sample()
+        except Exception:
+            return None
+        return sample
+
+    def _smi_sampler(self):
+        q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+        def sample():
+            out = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                  "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                 timeout=5).stdout.strip()
+            v = [x.strip() for x in out.split(",")]
+            num = lambda x: float(x) if x.replace(".", "").isdigit() else None
+            return num(v[0]), num(v[1]), {n: v[2 + i] == "Active" for i, n in enumerate(self._NAMES) if len(v) > 2 + i}
+
+        return sample
+
     def __enter__(self):
+        sample = self._nvml_sampler()
+        self.source, period = ("nvml", 0.01) if sample else ("nvidia-smi", 0.2)
+        if sample is None:
+            sample = self._smi_sampler()
+
         def run():
-            q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
-                 "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
-                 "clocks_event_reasons.sw_power_cap")
             while not self._stop.is_set():
                 try:
-                    out = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
-                                          "--format=csv,noheader,nounits"], capture_output=True, text=True,
-                                         timeout=5).stdout.strip()
-                    if out:
-                        self.rows.append([v.strip() for v in out.split(",")])
+                    self.rows.append(sample())
                 except Exception:
                     pass
-                self._stop.wait(0.2)
+                self._stop.wait(period)
 
         self._t = threading.Thread(target=run, daemon=True)
         self._t.start()
@@ -106,12 +145,12 @@ class Clocks:
     def summary(self):
         if not self.rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
-        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in self.rows for i in range(4) if len(r) > 3 + i and r[3 + i] == "Active"})
+        sm = [r[0] for r in self.rows if r[0] is not None]
+        mx = [r[1] for r in self.rows if r[1] is not None]
+        reasons = sorted({n for r in self.rows for n, on in r[2].items() if on})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(self.rows)}
+                "sm_min_mhz": min(sm) if sm else None, "reasons": reasons, "samples": len(self.rows),
+                "source": self.source}
 
 
 _REF_CACHE = {}
@@ -605,7 +644,11 @@ def ours_arm(args):
 
     # e2e through the public API: host angles in, expectation values out
     def e2e_step():
-        res = sim.simulate_and_measure(script.record(ang_t), n, "expval", obs, False, dtype=dt, tune=tune)
+        if tune is None:
+            res = script.execute("expval", obs, args=(ang_t,), dtype=dt)
+        else:  # a non-default tile width is reachable only below Script
+            with sim.gc_paused():
+                res = sim.simulate_and_measure(script.record(ang_t), n, "expval", obs, False, dtype=dt, tune=tune)
         return res.cpu()
 
     for _ in range(max(1, args.warmup)):

@@ -88,15 +88,17 @@ class Script:
                     f"Batched initial_state must be 1D (broadcast) or 2D (one state per sample); got ndim={nd}."
                 )
         args = tuple(_as_arg(a) for a in args)
-        if in_axes is not None:
-            return self._execute_batched(type, obs, args, kwargs, tuple(in_axes), shots, key, initial_state,
-                                         fingerprint, dtype)
-        tape = self.record(*args, **kwargs)
-        n_qubits = self._n_qubits or simulation.infer_n_qubits(tape, obs)
-        use_density = simulation.has_noise(tape)
-        return simulation.simulate_and_measure(
-            tape, n_qubits, type, obs, use_density, shots=shots, key=key, initial_state=initial_state, dtype=dtype
-        )
+        with simulation.gc_paused():
+            if in_axes is not None:
+                return self._execute_batched(type, obs, args, kwargs, tuple(in_axes), shots, key, initial_state,
+                                             fingerprint, dtype)
+            tape = self.record(*args, **kwargs)
+            n_qubits = self._n_qubits or simulation.infer_n_qubits(tape, obs)
+            use_density = simulation.has_noise(tape)
+            return simulation.simulate_and_measure(
+                tape, n_qubits, type, obs, use_density, shots=shots, key=key, initial_state=initial_state,
+                dtype=dtype
+            )
 
     @staticmethod
     def _batch_size(args: tuple, in_axes: Tuple) -> int:

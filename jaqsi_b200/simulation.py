@@ -10,7 +10,9 @@ flow back to the circuit's arguments through a single
 """
 from __future__ import annotations
 
+import contextlib
 import ctypes
+import gc
 import math
 import threading
 from collections import OrderedDict
@@ -39,6 +41,29 @@ def infer_n_qubits(ops: List[Operation], obs: List[Operation]) -> int:
 def has_noise(tape: List[Operation]) -> bool:
     """Whether the tape holds a Kraus channel (jaqsi/simulation.py:49-62)."""
     return any(isinstance(op, KrausChannel) for op in tape)
+
+
+@contextlib.contextmanager
+def gc_paused():
+    """Pause Python's cyclic garbage collector for one circuit call.
+
+    Recording a circuit allocates a few thousand short-lived container objects
+    per call (ops, wire lists, angle views).  With the collector running they
+    survive its young-generation passes while the tape is alive, are promoted
+    into the oldest generation and every few calls trigger a full collection
+    of the whole heap (tens of milliseconds with torch loaded).  They are all
+    freed by reference counting when the call returns, so pausing the
+    collector for the call changes only the timing.  The previous state is
+    restored on exit (a collector that was already off stays off).
+    """
+    was = gc.isenabled()
+    if was:
+        gc.disable()
+    try:
+        yield
+    finally:
+        if was:
+            gc.enable()
 
 
 def _device() -> torch.device:
@@ -349,27 +374,31 @@ def _view_gather(values: list, device: torch.device) -> Optional[torch.Tensor]:
     through a single scatter instead of one select-backward per angle.
     """
     base = None
+    dtype = None
     pos, offs, fpos, fval = [], [], [], []
+    tensor = torch.Tensor
     for i, v in enumerate(values):
-        if isinstance(v, torch.Tensor):
+        if isinstance(v, tensor):
             b = v._base
-            if b is None or v.numel() != 1 or v.dtype != b.dtype or not b.is_floating_point():
-                return None
-            if base is None:
-                base = b
-                if not base.is_contiguous():
+            if b is not base:
+                # first tensor angle: the base is checked once
+                if base is not None or b is None or not b.is_floating_point() or not b.is_contiguous():
                     return None
-            elif b is not base:
+                base, dtype = b, b.dtype
+            if v.dtype is not dtype or v.numel() != 1:
                 return None
             pos.append(i)
-            offs.append(v.storage_offset() - base.storage_offset())
+            offs.append(v.storage_offset())
         else:
             fpos.append(i)
             fval.append(float(v))
     if base is None:
         return None
     flat = base.reshape(-1)
-    idx = torch.tensor(offs, dtype=torch.long).to(flat.device, non_blocking=True)
+    idx = torch.tensor(offs, dtype=torch.long)
+    if base.storage_offset():
+        idx -= base.storage_offset()
+    idx = idx.to(flat.device, non_blocking=True)
     vals = flat.index_select(0, idx).to(torch.float64)
     if not fpos:
         return vals.to(device)
