@@ -372,6 +372,37 @@ void emit_pass(std::ostringstream& o, const jq_plan* plan, const Schedule& s, in
     o << "\n";
     ++nstage;
   }
+  // The last stage stores its registers straight to global memory (skipping
+  // the shared-memory write-back and the tile copy-out) when its lowest lane
+  // bits hold the lowest tile bits, so that every 32-byte sector is written
+  // whole by one warp instruction: lanes 0-3 (complex64) or lanes 0-1
+  // (complex128) on tile bits 0-1 / 0, which are contiguous in global memory.
+  // The tile's logical index of a shared-memory offset is its swizzle (an
+  // XOR-linear involution) and the global offset of a logical index is the
+  // deposit of its bits (also XOR-linear), so the global offset of register
+  // slot j is a per-thread base XOR a compile-time constant.
+  const Step& last = s.steps[pd.step_end - 1];
+  bool direct = t - rb >= 2 && c >= 2 &&
+                (c64 ? (last.tbits[0] == 1u && last.tbits[1] == 2u) : last.tbits[0] == 1u);
+  if (const char* e = std::getenv("JQ_JIT_DIRECT_STORE")) direct = direct && std::atoi(e) != 0;
+  const bool wide = nb > 31;
+  const char* OT = wide ? "u64" : "u32";
+  auto unswz = [&](uint64_t a) -> uint64_t {  // swz8 / swz16 of the device prelude (involutions)
+    if (c64) return a ^ (((a >> 4) ^ (a >> 8) ^ (a >> 12)) & 15u);
+    return a ^ (((a >> 3) ^ (a >> 6) ^ (a >> 9) ^ (a >> 12)) & 7u);
+  };
+  auto gdep = [&](uint64_t logical) -> uint64_t {  // global offset of a tile-local index
+    uint64_t g = 0;
+    for (int i = 0; i < t; ++i)
+      if ((logical >> i) & 1) g |= 1ULL << pd.bits[i];
+    return g;
+  };
+  if (direct) {
+    o << "  " << OT << " gt = 0;";
+    for (int i = 0; i < t - rb; ++i)
+      o << " if (tid & " << (1u << i) << "u) gt ^= " << gdep(unswz(last.tbits[i])) << (wide ? "ull;" : "u;");
+    o << "\n";
+  }
   const std::string tpl = "<" + std::to_string(t - rb) + ", " + std::to_string(t) + ", " + std::to_string(c) + ">";
   const std::string pf = (c64 ? "prefetch8t" : "prefetch16t") + tpl;
   o << "  const long long tiles_per = 1ll << " << (nb - t) << ";\n";
@@ -415,8 +446,26 @@ void emit_pass(std::ostringstream& o, const jq_plan* plan, const Schedule& s, in
     std::vector<int> var(nr);  // var[j]: variable holding amplitude j of the register block
     for (int j = 0; j < nr; ++j) var[j] = j;
     o << "    {\n";
-    for (int j = 0; j < nr; ++j) o << "      " << T << " v" << j << " = s[tb" << nstage << " ^ " << off[j] << "u];\n";
-    for (int ri = st.a; ri < st.b; ++ri) {
+    // Thread-controlled swaps of whole register halves (a permutation whose
+    // control is a thread bit and whose target is a register bit, with no
+    // register-bit control) at the head of the stage become part of the load
+    // address: slot j of a controlled thread loads slot j ^ 2^q1, i.e. the
+    // base offset moves by the offset of register bit q1.  The stores keep the
+    // unmoved base.
+    int ri0 = st.a;
+    std::string lbase = "tb" + std::to_string(nstage);
+    while (ri0 < st.b) {
+      const RegOp& ro = s.rops[ri0];
+      const uint32_t kind = ro.w0 & 15u, q1 = (ro.w0 >> 4) & 15u;
+      const uint32_t crm = ro.w1 & 0xFFu, ctm = (ro.w1 >> 8) & 0xFFFFu;
+      if (kind != RK_PERM1 || ctm == 0 || crm != 0) break;
+      if (ri0 == st.a) o << "      u32 tl = " << lbase << ";\n";
+      o << "      if ((tid & " << ctm << "u) == " << ctm << "u) tl ^= " << st.ebits[q1] << "u;\n";
+      lbase = "tl";
+      ++ri0;
+    }
+    for (int j = 0; j < nr; ++j) o << "      " << T << " v" << j << " = s[" << lbase << " ^ " << off[j] << "u];\n";
+    for (int ri = ri0; ri < st.b; ++ri) {
       const RegOp& ro = s.rops[ri];
       const uint32_t kind = ro.w0 & 15u, q1 = (ro.w0 >> 4) & 15u, q2 = (ro.w0 >> 8) & 15u;
       const uint32_t dk = (ro.w0 >> 12) & 15u, dq = ro.w0 >> 16;
@@ -512,11 +561,21 @@ void emit_pass(std::ostringstream& o, const jq_plan* plan, const Schedule& s, in
       }
       o << "      }\n";
     }
-    for (int j = 0; j < nr; ++j) o << "      s[tb" << nstage << " ^ " << off[j] << "u] = v" << var[j] << ";\n";
-    o << "    }\n    __syncthreads();\n";
+    if (direct && si == pd.step_end - 1) {
+      for (int j = 0; j < nr; ++j) {
+        uint64_t gj = gdep(unswz(off[j]));
+        o << "      __stcs(g + (gt ^ " << gj << (wide ? "ull" : "u") << "), v" << var[j] << ");\n";
+      }
+      o << "    }\n";
+    } else {
+      for (int j = 0; j < nr; ++j) o << "      s[tb" << nstage << " ^ " << off[j] << "u] = v" << var[j] << ";\n";
+      o << "    }\n    __syncthreads();\n";
+    }
     ++nstage;
   }
-  o << "    " << (c64 ? "store8t" : "store16t") << tpl << "(s, g, tbl);\n";
+  // (direct: the barrier below keeps the next prefetch out of this buffer
+  // until every warp has loaded its last stage)
+  if (!direct) o << "    " << (c64 ? "store8t" : "store16t") << tpl << "(s, g, tbl);\n";
   o << "    __syncthreads();\n";
   o << "  }\n}\n";
 }
