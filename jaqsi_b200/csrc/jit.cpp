@@ -304,7 +304,6 @@ std::string hex(uint64_t v) {
   return b;
 }
 
-// Emit the kernel of pass p (register-stage program only).
 // Straight-line bit deposit of `v` into the set bits of `mask`: one
 // shift-and-mask term per contiguous run of mask bits.
 std::string pdep_expr(const std::string& v, uint64_t mask) {
@@ -324,6 +323,81 @@ std::string pdep_expr(const std::string& v, uint64_t mask) {
   return e.empty() ? std::string("0ull") : "(" + e + ")";
 }
 
+// Split-complex form of a complex64 register stage.  Amplitudes are held in
+// pairs (v, v ^ sp) as R = (re_v, re_{v^sp}) and I = (im_v, im_{v^sp}), so a
+// one-qubit gate costs four packed FMAs per amplitude instead of six (no
+// re/im cross terms to recombine).  Valid when every gate and swap of the
+// stage maps the pairing onto itself: for each of its variable pairs (x, y)
+// the pair (x ^ sp, y ^ sp) is one of its pairs too, in the same roles, and x,
+// y sit in the same lane (the lane of v is the parity of v & lane_sel).
+struct SplitStage {
+  bool ok = false;
+  uint32_t sp = 0, lane_sel = 0;
+};
+
+static int parity32(uint32_t v) { return __builtin_popcount(v) & 1; }
+
+// rops [ri0, rb_end) of a stage with nr register slots; `dense_min` one-qubit
+// gates at least (the pack / unpack moves must pay off).
+static SplitStage plan_split(const Schedule& s, int ri0, int rb_end, int nr, int dense_min) {
+  SplitStage res;
+  std::vector<int> var(nr);
+  for (int j = 0; j < nr; ++j) var[j] = j;
+  std::vector<std::vector<std::pair<int, int>>> lists;  // ordered (x, y) pairs per gate / swap
+  std::vector<bool> ordered;
+  int ndense = 0;
+  for (int ri = ri0; ri < rb_end; ++ri) {
+    const RegOp& ro = s.rops[ri];
+    const uint32_t kind = ro.w0 & 15u, q1 = (ro.w0 >> 4) & 15u;
+    const uint32_t crm = ro.w1 & 0xFFu, ctm = (ro.w1 >> 8) & 0xFFFFu;
+    if (kind != RK_DENSE1 && kind != RK_PERM1) return res;
+    std::vector<std::pair<int, int>> pr;
+    for (int j = 0; j < nr; ++j) {
+      if ((j >> q1) & 1) continue;
+      if ((static_cast<uint32_t>(j) & crm) != crm) continue;
+      const int k = j | (1 << q1);
+      if (kind == RK_PERM1 && ctm == 0) std::swap(var[j], var[k]);
+      else pr.emplace_back(var[j], var[k]);
+    }
+    if (kind == RK_DENSE1) ++ndense;
+    if (!pr.empty()) {
+      lists.push_back(std::move(pr));
+      ordered.push_back(kind == RK_DENSE1);
+    }
+  }
+  if (ndense < dense_min) return res;
+  for (uint32_t sp = 1; sp < static_cast<uint32_t>(nr); ++sp) {
+    for (uint32_t ls = 1; ls < static_cast<uint32_t>(nr); ++ls) {
+      if (!parity32(ls & sp)) continue;
+      bool good = true;
+      for (size_t li = 0; li < lists.size() && good; ++li) {
+        const auto& L = lists[li];
+        for (const auto& xy : L) {
+          const uint32_t x = xy.first, y = xy.second;
+          if (parity32(ls & (x ^ y))) { good = false; break; }
+          bool found = false;
+          for (const auto& uv : L) {
+            const uint32_t u = uv.first, v = uv.second;
+            if ((u == (x ^ sp) && v == (y ^ sp)) || (!ordered[li] && u == (y ^ sp) && v == (x ^ sp))) {
+              found = true;
+              break;
+            }
+          }
+          if (!found) { good = false; break; }
+        }
+      }
+      if (good) {
+        res.ok = true;
+        res.sp = sp;
+        res.lane_sel = ls;
+        return res;
+      }
+    }
+  }
+  return res;
+}
+
+// Emit the kernel of pass p (register-stage program only).
 void emit_pass(std::ostringstream& o, const jq_plan* plan, const Schedule& s, int p, bool c64, int rb) {
   const PassDesc& pd = s.passes[p];
   const char* T = c64 ? "float2" : "double2";
@@ -336,6 +410,8 @@ void emit_pass(std::ostringstream& o, const jq_plan* plan, const Schedule& s, in
   if (const char* e = std::getenv("JQ_JIT_MINB")) minb = std::max(1, std::min(16, std::atoi(e)));
   // complex64 dense blocks use packed two-lane FMA unless JQ_JIT_SCALAR=1
   const bool packed = c64 && !(std::getenv("JQ_JIT_SCALAR") && std::atoi(std::getenv("JQ_JIT_SCALAR")) == 1);
+  // split-complex stages (see plan_split) with JQ_JIT_SPLIT=1
+  const bool split_on = packed && std::getenv("JQ_JIT_SPLIT") && std::atoi(std::getenv("JQ_JIT_SPLIT")) == 1;
   const uint64_t full = (nb >= 64) ? ~0ULL : ((1ULL << nb) - 1);
   const uint64_t outer = full & ~pd.tile_mask;
   const int smat_pad = (pd.smat_len + 1) & ~1;
@@ -465,6 +541,23 @@ void emit_pass(std::ostringstream& o, const jq_plan* plan, const Schedule& s, in
       ++ri0;
     }
     for (int j = 0; j < nr; ++j) o << "      " << T << " v" << j << " = s[" << lbase << " ^ " << off[j] << "u];\n";
+    const SplitStage sps = split_on ? plan_split(s, ri0, st.b, nr, 2) : SplitStage{};
+    auto is_lead = [&](int v) { return !parity32(sps.lane_sel & static_cast<uint32_t>(v)); };
+    std::vector<int> lead(nr);  // lane-0 variable of the pack holding variable v
+    if (sps.ok) {
+      for (int v = 0; v < nr; ++v) lead[v] = is_lead(v) ? v : (v ^ static_cast<int>(sps.sp));
+      for (int l = 0; l < nr; ++l)
+        if (is_lead(l))
+          o << "      float2 R" << l << " = make_float2(v" << l << ".x, v" << (l ^ sps.sp) << ".x), I" << l
+            << " = make_float2(v" << l << ".y, v" << (l ^ sps.sp) << ".y);\n";
+    }
+    // final value of register slot j
+    auto outv = [&](int j) -> std::string {
+      if (!sps.ok) return "v" + std::to_string(var[j]);
+      const int v = var[j], l = lead[v];
+      const std::string ln = (v == l) ? ".x" : ".y";
+      return "make_float2(R" + std::to_string(l) + ln + ", I" + std::to_string(l) + ln + ")";
+    };
     for (int ri = ri0; ri < st.b; ++ri) {
       const RegOp& ro = s.rops[ri];
       const uint32_t kind = ro.w0 & 15u, q1 = (ro.w0 >> 4) & 15u, q2 = (ro.w0 >> 8) & 15u;
@@ -472,6 +565,43 @@ void emit_pass(std::ostringstream& o, const jq_plan* plan, const Schedule& s, in
       const uint32_t crm = ro.w1 & 0xFFu, ctm = (ro.w1 >> 8) & 0xFFFFu, perm = ro.w1 >> 24;
       const uint32_t M = ro.w2;
       const bool guard = ctm != 0;
+      if (sps.ok) {  // plan_split admitted only one-qubit gates and swaps
+        if (guard) o << "      if ((tid & " << ctm << "u) == " << ctm << "u) {\n";
+        else o << "      {\n";
+        if (kind == RK_DENSE1) {
+          o << "        const float4* mq = (const float4*)smatb + " << M << ";\n";
+          o << "        const float4 A = mq[0], Bq = mq[1], Cq = mq[2], Dq = mq[3];\n";
+          o << "        const float2 ar = lo2(A), ai = hi2(A), br = lo2(Bq), bi = hi2(Bq), cr = lo2(Cq), ci = hi2(Cq), "
+               "dr = lo2(Dq), di = hi2(Dq);\n";
+          o << "        const float2 nai = make_float2(-ai.x, -ai.y), nbi = make_float2(-bi.x, -bi.y), "
+               "nci = make_float2(-ci.x, -ci.y), ndi = make_float2(-di.x, -di.y);\n";
+        }
+        for (int j = 0; j < nr; ++j) {
+          if ((j >> q1) & 1) continue;
+          if ((static_cast<uint32_t>(j) & crm) != crm) continue;
+          const int k = j | (1 << q1);
+          if (kind == RK_PERM1 && !guard) {
+            std::swap(var[j], var[k]);
+            continue;
+          }
+          const int x = var[j], y = var[k];
+          if (!is_lead(x)) continue;  // its pack is handled through the lane-0 pair
+          const std::string Rx = "R" + std::to_string(x), Ix = "I" + std::to_string(x);
+          const std::string Ry = "R" + std::to_string(y), Iy = "I" + std::to_string(y);
+          if (kind == RK_PERM1) {
+            o << "        { const float2 r = " << Rx << ", i = " << Ix << "; " << Rx << " = " << Ry << "; " << Ix << " = "
+              << Iy << "; " << Ry << " = r; " << Iy << " = i; }\n";
+            continue;
+          }
+          o << "        { const float2 rx = " << Rx << ", ix = " << Ix << ", ry = " << Ry << ", iy = " << Iy << ";\n";
+          o << "          " << Rx << " = __ffma2_rn(nbi, iy, __ffma2_rn(br, ry, __ffma2_rn(nai, ix, __fmul2_rn(ar, rx))));\n";
+          o << "          " << Ix << " = __ffma2_rn(bi, ry, __ffma2_rn(br, iy, __ffma2_rn(ai, rx, __fmul2_rn(ar, ix))));\n";
+          o << "          " << Ry << " = __ffma2_rn(ndi, iy, __ffma2_rn(dr, ry, __ffma2_rn(nci, ix, __fmul2_rn(cr, rx))));\n";
+          o << "          " << Iy << " = __ffma2_rn(di, ry, __ffma2_rn(dr, iy, __ffma2_rn(ci, rx, __fmul2_rn(cr, ix)))); }\n";
+        }
+        o << "      }\n";
+        continue;
+      }
       if (guard) o << "      if ((tid & " << ctm << "u) == " << ctm << "u) {\n";
       else o << "      {\n";
       auto V = [&](int j) { return std::string("v") + std::to_string(var[j]); };
@@ -564,11 +694,11 @@ void emit_pass(std::ostringstream& o, const jq_plan* plan, const Schedule& s, in
     if (direct && si == pd.step_end - 1) {
       for (int j = 0; j < nr; ++j) {
         uint64_t gj = gdep(unswz(off[j]));
-        o << "      __stcs(g + (gt ^ " << gj << (wide ? "ull" : "u") << "), v" << var[j] << ");\n";
+        o << "      __stcs(g + (gt ^ " << gj << (wide ? "ull" : "u") << "), " << outv(j) << ");\n";
       }
       o << "    }\n";
     } else {
-      for (int j = 0; j < nr; ++j) o << "      s[tb" << nstage << " ^ " << off[j] << "u] = v" << var[j] << ";\n";
+      for (int j = 0; j < nr; ++j) o << "      s[tb" << nstage << " ^ " << off[j] << "u] = " << outv(j) << ";\n";
       o << "    }\n    __syncthreads();\n";
     }
     ++nstage;
