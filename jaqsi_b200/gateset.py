@@ -225,6 +225,7 @@ def _make_rotation_gate(pauli_class, name: str, kind: int):
         is_unitary = True
         _param_names = ("theta",)
         _structure = GateStructure(diagonal=pauli_class is PauliZ)
+        _jq_param_kind = kind  # lowering fixed by the class (simulation._class_lowering)
 
         def __init__(self, theta, wires: Union[int, List[int]] = 0, **kwargs) -> None:
             self.theta = theta
@@ -349,6 +350,7 @@ class Rot(Operation):
     _num_wires = 1
     is_unitary = True
     _param_names = ("phi", "theta", "omega")
+    _jq_param_kind = L.JQ_K_ROT  # lowering fixed by the class (simulation._class_lowering)
 
     def __init__(self, phi, theta, omega, wires: Union[int, List[int]] = 0, **kwargs) -> None:
         self.phi = phi

@@ -210,25 +210,85 @@ def _is_tensor(v) -> bool:
     return isinstance(v, torch.Tensor)
 
 
+_CLASS_LOWERING: Dict[type, object] = {}
+
+
+def _class_lowering(cls):
+    """Lowering fields fixed by the op's class alone, or False.
+
+    Two kinds of class qualify: parametrised gates that declare
+    ``_jq_param_kind`` in their own class body (angles = their parameters in
+    ``_param_names`` order, no payload), and gates whose matrix is a
+    class-level constant with the default ``_jq_lower`` / ``_jq_static_key``.
+    Either way an instance that keeps the class's matrix and structure lowers
+    to (kind, static key, structure, unitary, parameter names, payload), and
+    only its wires and angle values vary.  "skip" marks barriers.
+    """
+    if issubclass(cls, Barrier):
+        return "skip"
+    kind = cls.__dict__.get("_jq_param_kind")
+    if kind is not None:
+        return (kind, (kind,), cls._structure, bool(cls.is_unitary), tuple(cls._param_names), None)
+    m = cls._matrix
+    if (m is not None and not isinstance(m, torch.Tensor) and cls._jq_lower is Operation._jq_lower
+            and cls._jq_static_key is Operation._jq_static_key):
+        c = cls.__dict__.get("_jq_const")
+        if c is None:
+            c = np.asarray(m, dtype=np.complex128)
+            cls._jq_const = c
+        return (L.JQ_K_CONST, (cls.__name__,), cls._structure, bool(cls.is_unitary), (), c)
+    return False
+
+
+def _bad_wire(op, wires, n_qubits):
+    bad = [w for w in wires if not (0 <= w < n_qubits)][0]
+    return ValueError(f"{op.name}: wire {bad} outside 0..{n_qubits - 1}")
+
+
 def lower_tape(tape: Sequence[Operation], n_qubits: int) -> Lowered:
     """Lower recorded ops to plan statics and per-call values."""
     lw = Lowered()
     keys = []
+    statics = lw.statics
     n_ang = 0
     n_mat = 0
     max_wires = L.JQ_MAX_OP_WIRES
     k_matrix, k_paulirot = L.JQ_K_MATRIX, L.JQ_K_PAULIROT
     tensor = torch.Tensor
     angles_out = lw.angles
+    valid = frozenset(range(n_qubits))
+    cache = _CLASS_LOWERING
     for op in tape:
-        if isinstance(op, Barrier):
+        cls = op.__class__
+        ent = cache.get(cls)
+        if ent is None:
+            ent = _class_lowering(cls)
+            cache[cls] = ent
+        if ent == "skip":
             continue
         wires = tuple(op._wires)
-        if wires and (min(wires) < 0 or max(wires) >= n_qubits):
-            bad = [w for w in wires if w < 0 or w >= n_qubits][0]
-            raise ValueError(f"{op.name}: wire {bad} outside 0..{n_qubits - 1}")
+        if not valid.issuperset(wires):
+            raise _bad_wire(op, wires, n_qubits)
         if len(wires) > max_wires:
             raise ValueError(f"{op.name}: gates on more than {max_wires} wires are not supported")
+        d = op.__dict__
+        if ent is not False and "_structure" not in d and "_matrix" not in d:
+            kind, skey, st, unitary, pnames, payload = ent
+            grad = 0
+            angle_slot = -1
+            if pnames:
+                angle_slot = n_ang
+                for nm in pnames:
+                    a = d[nm] if nm in d else getattr(op, nm)
+                    angles_out.append(a)
+                    if isinstance(a, tensor):
+                        grad = 1
+                n_ang += len(pnames)
+            keys.append((skey, wires, st, grad, unitary, 0))
+            statics.append((kind, wires, st, angle_slot, -1, 0, 0, 0, st.controls, payload, grad, unitary))
+            if not unitary:
+                lw.unitary = False
+            continue
         kind, angles, payload = op._jq_lower()
         st = op._structure
         unitary = bool(op.is_unitary)
@@ -256,7 +316,7 @@ def lower_tape(tape: Sequence[Operation], n_qubits: int) -> Lowered:
         pz = getattr(op, "_pz", 0)
         nctrl = getattr(op, "n_controls", 0) if kind == k_paulirot else st.controls
         keys.append((skey, wires, st, grad, unitary, mat_is_diag))
-        lw.statics.append((kind, wires, st, angle_slot, mat_slot, mat_is_diag, px, pz, nctrl, payload, grad, unitary))
+        statics.append((kind, wires, st, angle_slot, mat_slot, mat_is_diag, px, pz, nctrl, payload, grad, unitary))
         if not unitary:
             lw.unitary = False
     lw.key = tuple(keys)

@@ -183,3 +183,32 @@ def test_view_gather_matches_stack_and_gradient():
     # views of different tensors fall back to the stack
     other = torch.zeros(2, requires_grad=True)
     assert sim._view_gather([base[0, 0, 0], other[1]], torch.device("cpu")) is None
+
+
+def test_class_lowering_matches_generic(monkeypatch):
+    """The per-class lowering shortcut produces exactly what each op's own
+    _jq_lower / _jq_static_key give (plan key, statics, angle order)."""
+    rng = np.random.default_rng(11)
+    params = torch.linspace(0.1, 3.0, 3000, dtype=torch.float64, requires_grad=True)
+    with jq.recording() as tape:
+        random_circuit(7, 400, rng, params, channels=True)
+        jq.Barrier(wires=[0, 1])
+        jq.RX(0.25, wires=2)  # float angle: no gradient
+        jq.H(wires=0, matrix=np.eye(2))  # instance matrix: generic path
+    fast = sim.lower_tape(tape, 7)
+    monkeypatch.setattr(sim, "_CLASS_LOWERING", {})
+    monkeypatch.setattr(sim, "_class_lowering", lambda cls: "skip" if issubclass(cls, jq.Barrier) else False)
+    slow = sim.lower_tape(tape, 7)
+    assert fast.key == slow.key
+    assert len(fast.statics) == len(slow.statics) == len(tape) - 1
+    for a, b in zip(fast.statics, slow.statics):
+        for x, y in zip(a, b):
+            if isinstance(x, np.ndarray) or isinstance(y, np.ndarray):
+                np.testing.assert_array_equal(x, y)
+            elif isinstance(x, list):
+                assert len(x) == len(y) and all(np.array_equal(u, v) for u, v in zip(x, y))
+            else:
+                assert x == y
+    assert len(fast.angles) == len(slow.angles)
+    assert all(u is v for u, v in zip(fast.angles, slow.angles))
+    assert fast.unitary == slow.unitary
