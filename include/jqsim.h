@@ -128,8 +128,11 @@ typedef struct jq_tune {
   int32_t ckpt_stride;   /* passes between checkpoints of the checkpointed
                             reverse pass (0: ceil(sqrt(passes)))             */
   int32_t jit;           /* forward passes specialised per plan with NVRTC:
-                            0 auto (states of >= 2^16 amplitudes), 1 on,
-                            -1 off (register-stage interpreter only)          */
+                            0 auto (states of >= 2^16 amplitudes; if the
+                            specialisation fails the register-stage
+                            interpreter runs), 1 on (a failed specialisation
+                            fails every call on that device with its error
+                            text), -1 off (register-stage interpreter only)    */
 } jq_tune;
 
 /* Plan summary. */

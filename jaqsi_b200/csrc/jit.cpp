@@ -767,6 +767,31 @@ void emit_adj_pass(std::ostringstream& o, const jq_plan* plan, const Schedule& s
     o << "\n";
     ++nstage;
   }
+  // The stage run last (the pass's first step) stores psi and lambda straight
+  // to global memory under the same condition as the forward pass's last
+  // stage; the barrier at the top of the next tile keeps the next loads out
+  // of the tiles until every warp has read them.
+  const Step& fin = s.steps[pd.step_begin];
+  bool direct = t - rb >= 2 && c >= 2 &&
+                (c64 ? (fin.tbits[0] == 1u && fin.tbits[1] == 2u) : fin.tbits[0] == 1u);
+  if (const char* e = std::getenv("JQ_JIT_DIRECT_STORE")) direct = direct && std::atoi(e) != 0;
+  const bool wide = nb > 31;
+  auto unswz = [&](uint64_t v) -> uint64_t {
+    if (c64) return v ^ (((v >> 4) ^ (v >> 8) ^ (v >> 12)) & 15u);
+    return v ^ (((v >> 3) ^ (v >> 6) ^ (v >> 9) ^ (v >> 12)) & 7u);
+  };
+  auto gdep = [&](uint64_t logical) -> uint64_t {
+    uint64_t g = 0;
+    for (int i = 0; i < t; ++i)
+      if ((logical >> i) & 1) g |= 1ULL << pd.bits[i];
+    return g;
+  };
+  if (direct) {
+    o << "  " << (wide ? "u64" : "u32") << " gpos = 0;";
+    for (int i = 0; i < t - rb; ++i)
+      o << " if (tid & " << (1u << i) << "u) gpos ^= " << gdep(unswz(fin.tbits[i])) << (wide ? "ull;" : "u;");
+    o << "\n";
+  }
   // flush of the shared accumulators into the instance's global accumulator
   // (skipped when the caller wants no parameter gradient: gacc is NULL)
   auto flush_for = [&](const std::string& inst) {
@@ -965,13 +990,24 @@ void emit_adj_pass(std::ostringstream& o, const jq_plan* plan, const Schedule& s
       }
       o << "      }\n";
     }
-    for (int j = 0; j < nr; ++j)
-      o << "      sp[tb" << k << " ^ " << off[j] << "u] = p" << var[j] << "; sl[tb" << k << " ^ " << off[j]
-        << "u] = l" << var[j] << ";\n";
-    o << "    }\n    __syncthreads();\n";
+    if (direct && si == pd.step_begin) {
+      for (int j = 0; j < nr; ++j) {
+        const std::string gj = std::to_string(gdep(unswz(off[j]))) + (wide ? "ull" : "u");
+        o << "      __stcs(psi + goff + (gpos ^ " << gj << "), p" << var[j] << "); __stcs(lam + goff + (gpos ^ " << gj
+          << "), l" << var[j] << ");\n";
+      }
+      o << "    }\n";
+    } else {
+      for (int j = 0; j < nr; ++j)
+        o << "      sp[tb" << k << " ^ " << off[j] << "u] = p" << var[j] << "; sl[tb" << k << " ^ " << off[j]
+          << "u] = l" << var[j] << ";\n";
+      o << "    }\n    __syncthreads();\n";
+    }
   }
-  o << "    " << (c64 ? "store8t" : "store16t") << tpl << "(sp, psi + goff, tbl);\n";
-  o << "    " << (c64 ? "store8t" : "store16t") << tpl << "(sl, lam + goff, tbl);\n";
+  if (!direct) {
+    o << "    " << (c64 ? "store8t" : "store16t") << tpl << "(sp, psi + goff, tbl);\n";
+    o << "    " << (c64 ? "store8t" : "store16t") << tpl << "(sl, lam + goff, tbl);\n";
+  }
   o << "  }\n  __syncthreads();\n  if (last_inst >= 0) {\n" << flush_for("last_inst") << "  }\n}\n";
 }
 

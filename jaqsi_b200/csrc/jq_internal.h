@@ -150,6 +150,8 @@ struct DeviceTables {
   void* obs_desc = nullptr;       // DevObs array
   void* jit = nullptr;            // JitModule of the forward schedule (or nullptr)
   bool jit_tried = false;
+  int jit_rc = 0;                 // nonzero: the required specialisation failed
+  std::string jit_err;            // (its error text, returned by every later call)
 };
 
 struct DevObs {
@@ -187,5 +189,6 @@ struct jq_plan {
   int threads = 512;
   int ckpt_stride = 0;
   bool jit = false;             // specialise the forward passes with NVRTC
+  bool jit_required = false;    // jq_tune.jit = 1: a failed specialisation is an error
   std::vector<jq::DeviceTables> dev;  // per-device uploads
 };

@@ -1851,7 +1851,14 @@ int device_tables(const jq_plan* cplan, const DeviceTables** out) {
   JQ_CUDA(cudaGetDevice(&dev));
   std::lock_guard<std::mutex> lock(g_upload_mu);
   for (const DeviceTables& t : plan->dev)
-    if (t.device == dev) { *out = &t; return JQ_OK; }
+    if (t.device == dev) {
+      if (t.jit_rc) {
+        set_error(t.jit_err);
+        return t.jit_rc;
+      }
+      *out = &t;
+      return JQ_OK;
+    }
   DeviceTables t;
   t.device = dev;
   int rc;
@@ -1875,14 +1882,28 @@ int device_tables(const jq_plan* cplan, const DeviceTables** out) {
   if ((rc = upload(plan->bwd.rops, &t.bwd_rops))) return rc;
   if (plan->jit && jit_available()) {
     JitModule* jm = new JitModule();
-    if (jit_build(plan, plan->fwd, jm) == JQ_OK) {
+    if ((rc = jit_build(plan, plan->fwd, jm)) == JQ_OK) {
       t.jit = jm;
     } else {
-      delete jm;  // the interpreter kernels run instead
+      jit_free(jm);
+      delete jm;
+      // automatic mode: the register-stage interpreter kernels run instead;
+      // jq_tune.jit = 1: the plan fails on this device (tables kept for jq_plan_free)
+      if (plan->jit_required) {
+        t.jit_rc = rc;
+        t.jit_err = g_last_error;
+      }
     }
+  } else if (plan->jit_required) {
+    t.jit_rc = JQ_EUNSUPPORTED;
+    t.jit_err = "jq_tune.jit = 1 but NVRTC or the CUDA driver entry points are not available";
   }
   t.jit_tried = true;
   plan->dev.push_back(t);
+  if (t.jit_rc) {
+    set_error(t.jit_err);
+    return t.jit_rc;
+  }
   *out = &plan->dev.back();
   return JQ_OK;
 }

@@ -714,6 +714,7 @@ int build_plan(const jq_op* ops, int n_ops, const jq_obs* obs, int n_obs, int n_
     const char* env = std::getenv("JQ_NO_JIT");
     const bool env_off = env && env[0] && env[0] != '0';
     plan->jit = !env_off && (mode_jit > 0 || (mode_jit == 0 && nb >= 16));
+    plan->jit_required = !env_off && mode_jit > 0;
   }
 
   // ---- observables -----------------------------------------------------------------
