@@ -41,10 +41,10 @@ sys.path.insert(0, ROOT)
 METRIC = "adjoint grads/sec (batched) vs plain GPU sim at ≤1e-5 err; gate-pass HBM GB/s"
 N_QUBITS, LAYERS, SEED = 24, 20, 2
 # DRAM bytes per launch of the specialised tile pass, from one ncu capture
-# (--set full, 2 launches of the 24-qubit complex64 sweep): reads 134.3 MB
-# (the whole state once) + writes 74.3 / 75.4 MB (the rest of the write-back
+# (--set full, 2 launches of the 24-qubit complex64 sweep): reads 134.25 MB
+# (the whole state once) + writes 74.5 / 75.6 MB (the rest of the write-back
 # is still in the 126 MB L2 when the launch ends).
-TILE_PASS_TRAFFIC = {(24, "c64"): 209.1e6}
+TILE_PASS_TRAFFIC = {(24, "c64"): 209.3e6}
 
 
 def _peaks():
