@@ -212,3 +212,28 @@ def test_class_lowering_matches_generic(monkeypatch):
     assert len(fast.angles) == len(slow.angles)
     assert all(u is v for u, v in zip(fast.angles, slow.angles))
     assert fast.unitary == slow.unitary
+
+
+def test_gc_paused_restores_collector_state(monkeypatch):
+    """Script.execute pauses the cyclic collector only for the call, also when
+    the call raises, and leaves a collector that was off switched off."""
+    import gc
+
+    monkeypatch.setattr(torch.cuda, "is_available", lambda: False)
+    assert gc.isenabled()
+    seen = []
+
+    def circuit():
+        seen.append(gc.isenabled())
+        jq.H(0)
+
+    with pytest.raises(RuntimeError, match="CUDA"):
+        jq.Script(circuit, 1).execute("probs")
+    assert seen == [False] and gc.isenabled()
+    gc.disable()
+    try:
+        with sim.gc_paused():
+            assert not gc.isenabled()
+        assert not gc.isenabled()
+    finally:
+        gc.enable()
