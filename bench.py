@@ -81,6 +81,7 @@ class Clocks:
         self.source = None
         self._stop = threading.Event()
         self._t = None
+        self._nvml = None
 
     def _nvml_sampler(self):
         try:
@@ -102,7 +103,9 @@ class Clocks:
         try:
             sample()
         except Exception:
+            pynvml.nvmlShutdown()
             return None
+        self._nvml = pynvml
         return sample
 
     def _smi_sampler(self):
@@ -141,6 +144,12 @@ class Clocks:
         self._stop.set()
         if self._t:
             self._t.join(timeout=10)
+        if self._nvml is not None:
+            try:
+                self._nvml.nvmlShutdown()
+            except Exception:
+                pass
+            self._nvml = None
 
     def summary(self):
         if not self.rows:
