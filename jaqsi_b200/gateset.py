@@ -229,7 +229,10 @@ def _make_rotation_gate(pauli_class, name: str, kind: int):
 
         def __init__(self, theta, wires: Union[int, List[int]] = 0, **kwargs) -> None:
             self.theta = theta
-            super().__init__(wires=wires, **kwargs)
+            if kwargs or type(wires) is not int:
+                super().__init__(wires=wires, **kwargs)
+            else:  # one int wire, recorded: the circuit-recording hot path
+                self._record_fast([wires])
 
         @property
         def matrix(self) -> torch.Tensor:
@@ -274,7 +277,11 @@ def _make_controlled_gate(target_class, name: str):
         is_clifford = True
 
         def __init__(self, wires: List[int] = [0, 1], **kwargs) -> None:
-            super().__init__(wires=wires, **kwargs)
+            if kwargs or type(wires) is not list or len(wires) != 2 or type(wires[0]) is not int \
+                    or type(wires[1]) is not int or wires[0] == wires[1]:
+                super().__init__(wires=wires, **kwargs)  # (validates and raises)
+            else:  # two distinct int wires, recorded: the circuit-recording hot path
+                self._record_fast([wires[0], wires[1]])
 
         def decompose(self) -> List[Operation]:
             if name != "CZ":
@@ -356,7 +363,10 @@ class Rot(Operation):
         self.phi = phi
         self.theta = theta
         self.omega = omega
-        super().__init__(wires=wires, **kwargs)
+        if kwargs or type(wires) is not int:
+            super().__init__(wires=wires, **kwargs)
+        else:  # one int wire, recorded: the circuit-recording hot path
+            self._record_fast([wires])
 
     @property
     def matrix(self) -> torch.Tensor:

@@ -135,6 +135,16 @@ class Operation:
             if stack:
                 stack[-1].append(self)
 
+    def _record_fast(self, ws: List[int]) -> None:
+        """Common tail of ``__init__`` for subclasses' hot path: class name, no
+        instance matrix, recorded on the active tape.  *ws* is a fresh wire
+        list the caller has already validated."""
+        self.name = type(self).__name__
+        self._wires = ws
+        stack = getattr(_tape_local, "stack", None)
+        if stack:
+            stack[-1].append(self)
+
     # -- basic properties ----------------------------------------------------
     @property
     def wires(self) -> List[int]:
