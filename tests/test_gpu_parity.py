@@ -4,6 +4,9 @@ Tolerances (north star): 1e-10 in complex128 and 1e-5 in complex64 against
 the float64 oracle, for states, probabilities, densities, expectation values
 and gradients.
 """
+import json
+import os
+
 import numpy as np
 import pytest
 import torch
@@ -14,6 +17,8 @@ from oracle import sim_np as O
 from tests.helpers import ansatz_layers, count_params, obs_records, random_circuit, to_records
 
 pytestmark = pytest.mark.gpu
+KNOWN = json.load(open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden",
+                                    "reference_known_answers.json")))
 
 TOL = {torch.complex64: 1e-5, torch.complex128: 1e-10}
 DTYPES = [torch.complex64, torch.complex128]
@@ -182,14 +187,11 @@ def test_training_minimal_golden():
         loss.backward()
         return loss.item(), t.grad.numpy()
 
+    ka = KNOWN["minimal_training_loop"]
     losses, params = O.adam_trajectory(vg, np.array([0.1, 0.2]), 0.05, 100)
-    np.testing.assert_allclose(
-        losses[24:100:25],
-        [0.18954755673957352, -0.9329512143583855, -0.9923251517460319, -0.9999997904383473],
-        rtol=1e-12,
-    )
-    np.testing.assert_allclose(params[0], 3.1389723449742055, rtol=1e-12)
-    np.testing.assert_allclose(params[1], 0.2, atol=1e-8)
+    np.testing.assert_allclose(losses[24:100:25], ka["losses_24_100_25"], rtol=1e-12)
+    np.testing.assert_allclose(params[0], ka["param0_final"], rtol=1e-12)
+    np.testing.assert_allclose(params[1], ka["param1_final"], atol=1e-8)
 
 
 def test_training_fit_golden():
@@ -213,15 +215,12 @@ def test_training_fit_golden():
         loss.backward()
         return loss.item(), t.grad.numpy()
 
+    ka = KNOWN["fitting_data"]
     losses, weights = O.adam_trajectory(vg, np.array([0.1, 0.2]), 0.05, 100)
-    np.testing.assert_allclose(
-        losses[24:100:25],
-        [2.007329667037132e-07, 1.3095863100844179e-08, 1.0464218803546601e-11, 7.771503138489971e-14],
-        rtol=1e-12, atol=1e-15,
-    )
+    np.testing.assert_allclose(losses[24:100:25], ka["losses_24_100_25"], rtol=1e-12, atol=1e-15)
     # bounded absolutely: see tests/test_oracle.py::test_training_fit_trajectory
-    np.testing.assert_allclose(weights[0], -0.000856006429212641, rtol=0, atol=2e-14)
-    np.testing.assert_allclose(weights[1], 0.2, atol=1e-8)
+    np.testing.assert_allclose(weights[0], ka["param0_final"], rtol=0, atol=2e-14)
+    np.testing.assert_allclose(weights[1], ka["param1_final"], atol=1e-8)
 
 
 @pytest.mark.parametrize("dtype", DTYPES)

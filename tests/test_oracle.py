@@ -1,12 +1,20 @@
 """The CPU oracle against the reference's own known answers (no GPU needed).
 
-Every expected value below is copied from the reference's test suite (the
+The training trajectories come from tests/golden/reference_known_answers.json
+(extracted from the reference's test source by tests/golden/make_golden.py);
+every other expected value is copied from the reference's test suite (the
 file:line is given per test) or is the analytic answer that test asserts.
 """
+import json
+import os
+
 import numpy as np
 import pytest
 
 from oracle import sim_np as O
+
+KNOWN = json.load(open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden",
+                                    "reference_known_answers.json")))
 
 
 def _value_and_grad_minimal(p):
@@ -18,14 +26,11 @@ def _value_and_grad_minimal(p):
 
 def test_training_minimal_trajectory():
     """jaqsi/tests/test_training.py:33-66 (rtol 1e-12)."""
+    ka = KNOWN["minimal_training_loop"]
     losses, params = O.adam_trajectory(_value_and_grad_minimal, np.array([0.1, 0.2]), 0.05, 100)
-    np.testing.assert_allclose(
-        losses[24:100:25],
-        [0.18954755673957352, -0.9329512143583855, -0.9923251517460319, -0.9999997904383473],
-        rtol=1e-12,
-    )
-    np.testing.assert_allclose(params[0], 3.1389723449742055, rtol=1e-12)
-    np.testing.assert_allclose(params[1], 0.2, atol=1e-8)
+    np.testing.assert_allclose(losses[24:100:25], ka["losses_24_100_25"], rtol=1e-12)
+    np.testing.assert_allclose(params[0], ka["param0_final"], rtol=1e-12)
+    np.testing.assert_allclose(params[1], ka["param1_final"], atol=1e-8)
 
 
 def _value_and_grad_fit(w):
@@ -47,20 +52,16 @@ def _value_and_grad_fit(w):
 
 def test_training_fit_trajectory():
     """jaqsi/tests/test_training.py:69-106 (rtol 1e-12, atol 1e-15)."""
+    ka = KNOWN["fitting_data"]
     losses, weights = O.adam_trajectory(_value_and_grad_fit, np.array([0.1, 0.2]), 0.05, 100)
-    np.testing.assert_allclose(
-        losses[24:100:25],
-        [2.007329667037132e-07, 1.3095863100844179e-08, 1.0464218803546601e-11, 7.771503138489971e-14],
-        rtol=1e-12,
-        atol=1e-15,
-    )
+    np.testing.assert_allclose(losses[24:100:25], ka["losses_24_100_25"], rtol=1e-12, atol=1e-15)
     # weights[0] ~ -8.6e-4 accumulates 100 Adam steps of size ~lr whose late
     # gradients are O(1e-7) differences of O(1) numbers: merely reordering the
     # 16-sample gradient sum moves it by ~3e-15, so it is bounded absolutely
     # (2e-14, ~1e-16 of the O(1) quantities it is computed from) where the
     # reference's rtol=1e-12 would mean 9e-16.
-    np.testing.assert_allclose(weights[0], -0.000856006429212641, rtol=0, atol=2e-14)
-    np.testing.assert_allclose(weights[1], 0.2, atol=1e-8)
+    np.testing.assert_allclose(weights[0], ka["param0_final"], rtol=0, atol=2e-14)
+    np.testing.assert_allclose(weights[1], ka["param1_final"], atol=1e-8)
 
 
 BELL = [("H", [0], []), ("CX", [0, 1], [])]
