@@ -1,6 +1,6 @@
 """GPU parity: libjqsim (through Script / the C ABI) against the CPU oracle.
 
-Tolerances (north star): 1e-10 in complex128 and 1e-5 in complex64 against
+Tolerances: 1e-10 in complex128 and 1e-5 in complex64 against
 the float64 oracle, for states, probabilities, densities, expectation values
 and gradients.
 """
