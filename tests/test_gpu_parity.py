@@ -377,6 +377,24 @@ def test_specialised_equals_interpreter(dtype):
     np.testing.assert_allclose(_np(a), _np(b), atol=TOL[dtype])
 
 
+def test_split_complex_stages_equal_interpreter(monkeypatch):
+    """The optional split-complex register stages (JQ_JIT_SPLIT=1: pairs of
+    amplitudes held as (re, re) / (im, im) lanes) against the interpreter,
+    complex64, 20 qubits.  The distinct ckpt_stride keeps this plan out of
+    the cache entries of the default specialisation."""
+    n, layers = 20, 4
+    ang = np.random.default_rng(9).uniform(0, 2 * np.pi, (layers, n, 3))
+    with jq.recording() as tape:
+        ansatz_layers(n, layers, ang)
+        jq.CRX(0.3, wires=[5, 14])
+    monkeypatch.setenv("JQ_JIT_SPLIT", "1")
+    a = sim.simulate_and_measure(tape, n, "state", [], False, dtype=torch.complex64,
+                                 tune={"jit": 1, "ckpt_stride": 7})
+    monkeypatch.delenv("JQ_JIT_SPLIT")
+    b = sim.simulate_and_measure(tape, n, "state", [], False, dtype=torch.complex64, tune={"jit": -1})
+    np.testing.assert_allclose(_np(a), _np(b), atol=TOL[torch.complex64])
+
+
 @pytest.mark.parametrize("dtype", DTYPES)
 def test_specialised_adjoint_matches_oracle(dtype):
     """The NVRTC-specialised adjoint passes (the forward schedule run backwards,
