@@ -237,3 +237,58 @@ def test_gc_paused_restores_collector_state(monkeypatch):
         assert not gc.isenabled()
     finally:
         gc.enable()
+
+
+def _jit_source(plan):
+    n = plan._lib.jq_plan_jit_source(plan.handle, None, 0)
+    buf = ctypes.create_string_buffer(n + 1)
+    plan._lib.jq_plan_jit_source(plan.handle, buf, n + 1)
+    return buf.value.decode()
+
+
+def test_direct_store_addresses_match_tile_layout():
+    """Specialised passes whose last register stage stores straight to global
+    memory (forward: gt, adjoint: gpos) must write every register slot where
+    the shared-memory tile copy-out would have put it: global offset =
+    deposit(unswizzle(shared-memory offset)).  Checked on the emitted source
+    of a 20-qubit complex64 plan (no GPU needed)."""
+    n, layers = 20, 4
+    ang = np.random.default_rng(12).uniform(0, 2 * np.pi, (layers, n, 3))
+    with jq.recording() as tape:
+        ansatz_layers(n, layers, ang)
+    plan = _plan(tape, n, obs=[jq.PauliZ(0)], dtype=torch.complex64, tune={"jit": 1})
+    src = _jit_source(plan)
+    kernels = re.split(r'extern "C" __global__', src)[1:]
+    assert kernels
+    unswz = lambda a: a ^ (((a >> 4) ^ (a >> 8) ^ (a >> 12)) & 15)
+    checked = {"fwd": 0, "adj": 0}
+    for k in kernels:
+        hb = [int(x) for x in re.search(r"const u32 hb\[\] = \{([^}]*)\}", k).group(1).split(",")]
+        cb = int(re.search(r"prefetch8t<\d+, \d+, (\d+)>", k).group(1))
+
+        def gdep(logical):
+            g = 0
+            for i in range(cb + len(hb)):
+                if (logical >> i) & 1:
+                    g |= (1 << i) if i < cb else hb[i - cb]
+            return g
+
+        adj = "lam" in k.split("{", 1)[0]
+        base = "gpos" if adj else "gt"
+        gline = re.search(r"u32 %s = 0;(.*)" % base, k)
+        if gline is None:
+            assert "__stcs(g + " not in k and "__stcs(psi + " not in k
+            continue
+        tbs = re.findall(r"u32 tb(\d+) = 0;(.*)", k)
+        # forward: the last stage stores; adjoint: stage 0 (run last)
+        tb_line = tbs[0][1] if adj else tbs[-1][1]
+        tbits = [int(x) for x in re.findall(r"\^= (\d+)u;", tb_line)]
+        gbits = [int(x) for x in re.findall(r"\^= (\d+)u;", gline.group(1))]
+        assert gbits == [gdep(unswz(t)) for t in tbits]
+        loads = re.findall(r"float2 %s(\d+) = %s\[\w+ \^ (\d+)u\];" % (("p", "sp") if adj else ("v", "s")), k)
+        nr = 1 << (max(int(j) for j, _ in loads).bit_length())
+        off = [int(o) for _, o in loads[-nr:]]
+        stores = [int(y) for y in re.findall(r"__stcs\(%s \+ \(%s \^ (\d+)u\)" % ("psi \\+ goff" if adj else "g", base), k)]
+        assert stores == [gdep(unswz(o)) for o in off]
+        checked["adj" if adj else "fwd"] += 1
+    assert checked["fwd"] > 0 and checked["adj"] > 0
