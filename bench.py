@@ -259,6 +259,7 @@ def _config(args, p_ref, p_ours):
                     f"wire + CX ring, expval of Z_iZ_(i+1) (open chain)",
         "n_qubits": N_QUBITS, "layers": LAYERS, "seed": SEED, "dtype": args.dtype,
         "reference_plan_passes": p_ref, "our_passes": p_ours,
+        "unfused_passes": LAYERS * 4 * N_QUBITS,  # one pass per recorded gate
         "value_def": "reference-plan passes x 2 x 2^n x elem bytes / step time",
         "l2": "flushed between timed steps (256 MiB write); state 128 MiB (c64) / 256 MiB (c128)",
         "parallelism": f"replicas x{args.gpus}",
