@@ -228,7 +228,8 @@ JQ_API int jq_sweep(const jq_plan* plan, int batch, const double* angles,
  * (one prior jq_forward / jq_adjoint / jq_backward / jq_sweep on that device),
  * otherwise JQ_EINVAL.  The first call on a device resolves the array's
  * address (cudaGetSymbolAddress); make that first call before any stream
- * capture.  All calls share the array and it keeps the last call's contents,
+ * capture (a first call made while `stream` is capturing returns JQ_EINVAL
+ * and does nothing).  All calls share the array and it keeps the last call's contents,
  * so calls that overlap on the GPU (other streams, other threads) race:
  * serialise them.  Arguments and results are those of jq_forward. */
 #define JQ_STATIC_WS_BYTES (4u << 20)

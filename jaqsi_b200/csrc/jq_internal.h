@@ -5,6 +5,7 @@
 #include <array>
 #include <cstdint>
 #include <string>
+#include <deque>
 #include <vector>
 
 #include "../../include/jqsim.h"
@@ -190,5 +191,5 @@ struct jq_plan {
   int ckpt_stride = 0;
   bool jit = false;             // specialise the forward passes with NVRTC
   bool jit_required = false;    // jq_tune.jit = 1: a failed specialisation is an error
-  std::vector<jq::DeviceTables> dev;  // per-device uploads
+  std::deque<jq::DeviceTables> dev;  // per-device uploads (a deque: references stay valid as devices are added)
 };

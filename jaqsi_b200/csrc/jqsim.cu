@@ -1951,6 +1951,9 @@ WsLayout layout(const jq_plan* plan, int batch, int mode_grad /*0 fwd, 1 adjoint
   return L;
 }
 
+// Largest grid.y of a launch (instances of a batch run along y).
+constexpr int kMaxGridY = 65535;
+
 int grid_for(int64_t work, int threads) {
   int64_t g = (work + threads - 1) / threads;
   const int64_t cap = static_cast<int64_t>(sm_count()) * 16;
@@ -2082,18 +2085,27 @@ int measure(const jq_plan* plan, const DeviceTables* T, int batch, int out_type,
           ++j;
         const int gx = std::max(1, std::min<int>(static_cast<int>((dim + threads - 1) / threads),
                                                  std::max(1, 4 * sm_count() / std::max(batch, 1))));
-        dim3 grid(gx, batch);
-        if (dm) k_expval_pauli_dm<R><<<grid, threads, 0, st>>>(state, dim, od, i, j - i, o, n_obs);
-        else if (zdiag) k_expval_zdiag_sv<R><<<grid, threads, 0, st>>>(state, dim, od, i, j - i, o, n_obs);
-        else k_expval_pauli_sv<R><<<grid, threads, 0, st>>>(state, dim, od, i, j - i, o, n_obs);
+        // instances run along grid.y, at most kMaxGridY per launch
+        for (int b0 = 0; b0 < batch; b0 += kMaxGridY) {
+          const dim3 grid(gx, std::min(batch - b0, kMaxGridY));
+          const C* sb = state + static_cast<int64_t>(b0) * plan->state_elems;
+          double* ob = o + static_cast<int64_t>(b0) * n_obs;
+          if (dm) k_expval_pauli_dm<R><<<grid, threads, 0, st>>>(sb, dim, od, i, j - i, ob, n_obs);
+          else if (zdiag) k_expval_zdiag_sv<R><<<grid, threads, 0, st>>>(sb, dim, od, i, j - i, ob, n_obs);
+          else k_expval_pauli_sv<R><<<grid, threads, 0, st>>>(sb, dim, od, i, j - i, ob, n_obs);
+        }
         i = j;
       } else {
         const int64_t groups = dim >> plan->obs[i].k;
         const int gx = std::max(1, std::min<int>(static_cast<int>((groups + threads - 1) / threads),
                                                  std::max(1, 4 * sm_count() / std::max(batch, 1))));
-        dim3 grid(gx, batch);
-        if (dm) k_expval_dense_dm<R><<<grid, threads, 0, st>>>(state, n, od, i, pool, o, n_obs);
-        else k_expval_dense_sv<R><<<grid, threads, 0, st>>>(state, n, od, i, pool, o, n_obs);
+        for (int b0 = 0; b0 < batch; b0 += kMaxGridY) {
+          const dim3 grid(gx, std::min(batch - b0, kMaxGridY));
+          const C* sb = state + static_cast<int64_t>(b0) * plan->state_elems;
+          double* ob = o + static_cast<int64_t>(b0) * n_obs;
+          if (dm) k_expval_dense_dm<R><<<grid, threads, 0, st>>>(sb, n, od, i, pool, ob, n_obs);
+          else k_expval_dense_sv<R><<<grid, threads, 0, st>>>(sb, n, od, i, pool, ob, n_obs);
+        }
         ++i;
       }
     }
@@ -2673,7 +2685,10 @@ int jq_forward_noalloc(const jq_plan* plan, int batch, const double* angles, con
     return JQ_ECUDA;
   }
   bool resident = false;
-  for (const DeviceTables& t : plan->dev) resident = resident || t.device == dev;
+  {
+    std::lock_guard<std::mutex> lock(g_upload_mu);  // device_tables() appends under this lock
+    for (const DeviceTables& t : plan->dev) resident = resident || t.device == dev;
+  }
   if (!resident) {
     set_error("jq_forward_noalloc: the plan is not resident on this device; run jq_forward (or another "
               "execution entry point) with it once on this device first");
@@ -2692,6 +2707,15 @@ int jq_forward_noalloc(const jq_plan* plan, int batch, const double* angles, con
     for (const auto& e : g_noalloc_ptr)
       if (e.first == dev) ws = e.second;
     if (!ws) {
+      // the address is resolved once per device, and not inside a stream
+      // capture (the runtime call is not part of what a capture records)
+      cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+      if (cudaStreamIsCapturing(static_cast<cudaStream_t>(stream), &cap) != cudaSuccess ||
+          cap != cudaStreamCaptureStatusNone) {
+        set_error("jq_forward_noalloc: the first call on a device resolves the static workspace address and "
+                  "must not run inside a stream capture; call it once on this device outside the capture first");
+        return JQ_EINVAL;
+      }
       const cudaError_t e = cudaGetSymbolAddress(&ws, g_noalloc_ws);
       if (e != cudaSuccess || !ws) {
         set_error(std::string("jq_forward_noalloc: cudaGetSymbolAddress failed: ") + cudaGetErrorString(e));

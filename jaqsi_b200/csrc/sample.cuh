@@ -21,9 +21,9 @@ __device__ __forceinline__ uint64_t splitmix64(uint64_t x) {
 // tile total goes to bsum[row * ntiles + tile].
 __global__ void __launch_bounds__(kScanThreads) k_scan_tiles(const double* __restrict__ p, int64_t dim,
                                                              double* __restrict__ cdf, double* __restrict__ bsum,
-                                                             int64_t ntiles) {
+                                                             int64_t ntiles, int64_t row0) {
   __shared__ double warp_tot[kScanThreads / 32];
-  const int64_t row = blockIdx.y;
+  const int64_t row = row0 + blockIdx.y;
   const int64_t base = row * dim + static_cast<int64_t>(blockIdx.x) * kScanTile;
   const int64_t lim = dim - static_cast<int64_t>(blockIdx.x) * kScanTile;
   double v[kScanPer];
@@ -88,8 +88,9 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_totals(double* __restrict
   }
 }
 
-__global__ void k_scan_add(double* __restrict__ cdf, int64_t dim, const double* __restrict__ bsum, int64_t ntiles) {
-  const int64_t row = blockIdx.y;
+__global__ void k_scan_add(double* __restrict__ cdf, int64_t dim, const double* __restrict__ bsum, int64_t ntiles,
+                           int64_t row0) {
+  const int64_t row = row0 + blockIdx.y;
   const double add = bsum[row * ntiles + blockIdx.x];
   const int64_t base = row * dim + static_cast<int64_t>(blockIdx.x) * kScanTile;
   const int64_t lim = dim - static_cast<int64_t>(blockIdx.x) * kScanTile;
@@ -99,8 +100,8 @@ __global__ void k_scan_add(double* __restrict__ cdf, int64_t dim, const double* 
 // One draw per shot: u uniform in [0, total), the smallest i with
 // cdf[i] > u (a zero-probability index is never chosen).
 __global__ void k_sample(const double* __restrict__ cdf, int64_t dim, int64_t shots, uint64_t seed,
-                         uint32_t* __restrict__ counts) {
-  const int64_t row = blockIdx.y;
+                         uint32_t* __restrict__ counts, int64_t row0) {
+  const int64_t row = row0 + blockIdx.y;
   const double* c = cdf + row * dim;
   const double total = c[dim - 1];
   if (!(total > 0.0)) return;
@@ -130,14 +131,23 @@ int sample_impl(const double* probs, int batch, int64_t dim, int64_t shots, uint
   double* cdf = static_cast<double*>(ws);
   double* bsum = cdf + static_cast<int64_t>(batch) * dim;
   JQ_CUDA(cudaMemsetAsync(counts, 0, sizeof(uint32_t) * static_cast<size_t>(batch) * dim, st));
-  const dim3 g(static_cast<unsigned>(ntiles), static_cast<unsigned>(batch));
-  k_scan_tiles<<<g, kScanThreads, 0, st>>>(probs, dim, cdf, bsum, ntiles);
+  // rows run along grid.y, at most kMaxGridY per launch (row0 keeps each
+  // row's index, and so its random stream, whatever the slicing)
+  for (int b0 = 0; b0 < batch; b0 += kMaxGridY) {
+    const dim3 g(static_cast<unsigned>(ntiles), static_cast<unsigned>(std::min(batch - b0, kMaxGridY)));
+    k_scan_tiles<<<g, kScanThreads, 0, st>>>(probs, dim, cdf, bsum, ntiles, b0);
+  }
   k_scan_totals<<<batch, kScanThreads, 0, st>>>(bsum, ntiles);
-  k_scan_add<<<g, kScanThreads, 0, st>>>(cdf, dim, bsum, ntiles);
+  for (int b0 = 0; b0 < batch; b0 += kMaxGridY) {
+    const dim3 g(static_cast<unsigned>(ntiles), static_cast<unsigned>(std::min(batch - b0, kMaxGridY)));
+    k_scan_add<<<g, kScanThreads, 0, st>>>(cdf, dim, bsum, ntiles, b0);
+  }
   if (shots > 0) {
     const int64_t gx = std::max<int64_t>(1, std::min<int64_t>((shots + 255) / 256, 4 * sm_count()));
-    k_sample<<<dim3(static_cast<unsigned>(gx), static_cast<unsigned>(batch)), 256, 0, st>>>(cdf, dim, shots, seed,
-                                                                                            counts);
+    for (int b0 = 0; b0 < batch; b0 += kMaxGridY) {
+      const dim3 g(static_cast<unsigned>(gx), static_cast<unsigned>(std::min(batch - b0, kMaxGridY)));
+      k_sample<<<g, 256, 0, st>>>(cdf, dim, shots, seed, counts, b0);
+    }
   }
   JQ_CUDA(cudaGetLastError());
   return JQ_OK;

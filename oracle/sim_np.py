@@ -441,6 +441,41 @@ def jaqsi_mixed_pass_count(records, n: int) -> int:
     return len(fuse(superops))
 
 
+def jaqsi_mixed_plan(records, n: int) -> List[Tuple[str, Tuple[int, ...], np.ndarray]]:
+    """Fused superoperator blocks of jaqsi's _compile_mixed (:348-381) with
+    their matrices, as ('dense', axes, S) entries on the 2n-axis density
+    vector: sum_k kron(K, K*) for a channel, kron(U, U*) for a gate on at most
+    two wires, U on the ket axes and U* on the bra axes for wider gates; then
+    _fuse (:214-240) multiplies neighbours on identical axis tuples."""
+    blocks: List[list] = []
+    last: Dict[int, int] = {}
+
+    def push(S, axes):
+        i = last.get(axes[0])
+        if i is not None and blocks[i][1] == axes and all(last.get(a) == i for a in axes):
+            blocks[i][0] = S @ blocks[i][0]
+            return
+        blocks.append([S, axes])
+        for a in axes:
+            last[a] = len(blocks) - 1
+
+    for name, wires, params in records:
+        if name == "Barrier":
+            continue
+        ket = tuple(wires)
+        bra = tuple(w + n for w in wires)
+        if name in CHANNELS:
+            push(sum(np.kron(K, K.conj()) for K in kraus(name, params)), ket + bra)
+        else:
+            U = gate_matrix(name, params, len(wires))
+            if len(ket) <= 2:
+                push(np.kron(U, U.conj()), ket + bra)
+            else:
+                push(U, ket)
+                push(U.conj(), bra)
+    return [("dense", axes, S) for S, axes in blocks]
+
+
 # ---------------------------------------------------------------------------
 # optax.adam restated (defaults of optax 0.2.8)
 # ---------------------------------------------------------------------------
@@ -523,9 +558,12 @@ def compose_permutation(blocks, n: int) -> np.ndarray:
     return index.astype(np.int32)
 
 
-def jaqsi_plan(records, n: int):
+def jaqsi_plan(records, n: int, compose=None):
     """Entries ('dense', wires, U) | ('gather', index) | ('diag', wires, d) of
-    jaqsi's statevector plan: _fuse then _fuse_runs."""
+    jaqsi's statevector plan: _fuse then _fuse_runs.  ``compose(run, n)``
+    builds a permutation run's gather map (default: compose_permutation;
+    oracle/cplan.py passes the C version of the same fold)."""
+    compose = compose or compose_permutation
     blocks: List[list] = []
     last: Dict[int, int] = {}
     for name, wires, params in records:
@@ -548,7 +586,7 @@ def jaqsi_plan(records, n: int):
 
     def flush():
         if len(run) > 1 and kind == "perm":
-            plan.append(("gather", compose_permutation(run, n)))
+            plan.append(("gather", compose(run, n)))
         elif len(run) > 1:
             ws = tuple(sorted({w for b in run for w in b[1]}))
             d = np.ones((2,) * len(ws), dtype=np.complex128)

@@ -3,15 +3,16 @@
 * ``reference_known_answers.json``: the expected values that the reference's
   own training tests assert (jaqsi/tests/test_training.py:33-106), read from
   that file's source text with ``ast`` (the reference is not imported or run:
-  it needs JAX, which is not installed).  Needs the reference checkout at
-  /root/reference; the file is kept otherwise.
+  it needs JAX, which is not installed).  Needs the reference checkout: its
+  root is the first command-line argument, else $JAQSI_REFERENCE, else
+  /root/reference; without one the file is kept as it is.
 * ``oracle_vectors.npz``: seeded random circuits over the gate library (a
   noisy one included) with the float64 oracle's state / density,
   probabilities, expectation values and adjoint gradients.  The oracle is
   pinned by the known answers above (tests/test_oracle.py), and these vectors
   fix its outputs so the GPU parity tests compare against committed numbers.
 
-Run from the repository root:  python tests/golden/make_golden.py
+Run from the repository root:  python tests/golden/make_golden.py [REFERENCE_ROOT]
 """
 from __future__ import annotations
 
@@ -31,7 +32,11 @@ import jaqsi_b200 as jq  # noqa: E402
 from oracle import sim_np as O  # noqa: E402
 from tests.helpers import count_params, obs_records, random_circuit, to_records  # noqa: E402
 
-REFERENCE_TRAINING_TESTS = "/root/reference/tests/test_training.py"
+def reference_training_tests(root=None) -> str:
+    """The reference's training tests under `root`, else $JAQSI_REFERENCE,
+    else /root/reference."""
+    root = root or os.environ.get("JAQSI_REFERENCE", "/root/reference")
+    return os.path.join(root, "tests", "test_training.py")
 
 # name: (qubits, depth, seed, 3-qubit gates, channels)
 CASES = {
@@ -93,8 +98,8 @@ def _literal_values(fn: ast.FunctionDef):
     return lists, scalars
 
 
-def known_answers():
-    tree = ast.parse(open(REFERENCE_TRAINING_TESTS).read())
+def known_answers(path):
+    tree = ast.parse(open(path).read())
     fns = {n.name: n for n in tree.body if isinstance(n, ast.FunctionDef)}
     out = {"source": "jaqsi/tests/test_training.py"}
     for key, fname, lines in (("minimal_training_loop", "test_minimal_training_loop", "33-66"),
@@ -105,10 +110,11 @@ def known_answers():
     return out
 
 
-def main():
-    if os.path.exists(REFERENCE_TRAINING_TESTS):
+def main(root=None):
+    path = reference_training_tests(root)
+    if os.path.exists(path):
         with open(os.path.join(HERE, "reference_known_answers.json"), "w") as f:
-            json.dump(known_answers(), f, indent=1)
+            json.dump(known_answers(path), f, indent=1)
             f.write("\n")
     arrays = {}
     for name, (n, depth, seed, wide, channels) in CASES.items():
@@ -122,4 +128,4 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1] if len(sys.argv) > 1 else None)

@@ -445,3 +445,46 @@ def test_specialised_adjoint_equals_interpreter(dtype):
     tol = TOL[dtype]
     for a, b in zip(grads[0], grads[1]):
         np.testing.assert_allclose(a, b, atol=tol * 30)
+
+
+def test_batch_beyond_grid_y_limit():
+    """70,000 parameter sets in one call: the measurement and sampling kernels
+    run instances along grid.y, at most 65,535 per launch."""
+    import ctypes
+
+    from jaqsi_b200 import _lib as L
+
+    th = torch.linspace(0, 2 * np.pi, 70000, dtype=torch.float64)
+
+    def pure(t):
+        jq.RY(t, wires=0)
+        jq.CX(wires=[0, 1])
+
+    herm = jq.Hermitian(np.array([[0.5, 0.2], [0.2, -1.0]]), wires=1, record=False)
+    ev = jq.Script(pure, n_qubits=2).execute("expval", [jq.PauliZ(1), herm], args=(th,), in_axes=(0,))
+    c, s = np.cos(th.numpy() / 2) ** 2, np.sin(th.numpy() / 2) ** 2
+    np.testing.assert_allclose(_np(ev[:, 0]), c - s, atol=1e-12)
+    np.testing.assert_allclose(_np(ev[:, 1]), 0.5 * c - 1.0 * s, atol=1e-12)
+
+    def noisy(t):
+        jq.RX(t, wires=0)
+        jq.AmplitudeDamping(0.25, wires=0)
+
+    ev = jq.Script(noisy, n_qubits=1).execute("expval", [jq.PauliZ(0)], args=(th,), in_axes=(0,))
+    p1 = 0.75 * np.sin(th.numpy() / 2) ** 2
+    np.testing.assert_allclose(_np(ev[:, 0]), 1 - 2 * p1, atol=1e-12)
+
+    # shot sampling straight through the C ABI: row r puts all mass on r mod 4
+    batch, dim, shots = 70000, 4, 16
+    probs = torch.zeros((batch, dim), dtype=torch.float64, device="cuda")
+    probs[torch.arange(batch), torch.arange(batch) % dim] = 1.0
+    counts = torch.empty((batch, dim), dtype=torch.int32, device="cuda")
+    lib = L.lib()
+    wsb = lib.jq_sample_workspace_bytes(batch, dim)
+    ws = torch.empty(wsb, dtype=torch.uint8, device="cuda")
+    vp = ctypes.c_void_p
+    L.check(lib.jq_sample_shots(vp(probs.data_ptr()), batch, dim, shots, 7, vp(counts.data_ptr()), vp(ws.data_ptr()),
+                                wsb, vp(torch.cuda.current_stream().cuda_stream)))
+    want = torch.zeros_like(counts)
+    want[torch.arange(batch), torch.arange(batch) % dim] = shots
+    assert torch.equal(counts, want)

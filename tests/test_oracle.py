@@ -194,3 +194,44 @@ def test_mixed_matches_pure_for_unitaries():
     rho = O.simulate_mixed(recs + [("Matrix", [0], [np.eye(2)])], 3)
     np.testing.assert_allclose(rho, np.outer(psi, psi.conj()), atol=1e-12)
     del rng
+
+
+def _layered_records(n, layers, rng, noisy=False):
+    from jaqsi_b200 import workloads as W
+
+    ang = rng.uniform(0, 2 * np.pi, (layers, n, 3))
+    recs = W.noisy_ansatz_records(n, layers, ang) if noisy else W.sweep_ansatz_records(n, layers, ang)
+    if not noisy:
+        recs += W.strongly_entangling_records(n, 2, ang)
+        recs += [("CZ", [w, (w + 3) % n], []) for w in range(n)]
+        recs += [("CRX", [0, n - 2], [0.3]), ("SWAP", [1, n - 1], []), ("RZ", [2], [0.7]), ("RZ", [2], [0.2])]
+    else:
+        recs += [("CCX", [0, 2, 1], []), ("CRY", [1, 3], [0.4]), ("PhaseDamping", [2], [0.2])]
+    return recs
+
+
+@pytest.mark.parametrize("noisy", [False, True])
+def test_c_plan_runner_matches_numpy_oracle(noisy):
+    """oracle/jqoracle.c runs the reference's compiled plan (statevector:
+    dense / gather / diagonal entries; density: fused superoperators) and
+    must give the op-by-op NumPy oracle's state, in float64 and float32."""
+    from oracle import cplan
+
+    n = 4 if noisy else 9
+    recs = _layered_records(n, 3, np.random.default_rng(11), noisy)
+    want = O.simulate_mixed(recs, n).reshape(-1) if noisy else O.simulate_pure(recs, n)
+    plan = cplan.ReferencePlan(recs, n, mixed=noisy)
+    if noisy:
+        assert plan.passes == O.jaqsi_mixed_pass_count(recs, n)
+    else:
+        assert plan.passes == O.jaqsi_pass_count(recs)
+        assert {e[0] for e in plan.entries} == {"dense", "gather", "diag"}
+        numpy_maps = [e[1] for e in O.jaqsi_plan(recs, n) if e[0] == "gather"]
+        c_maps = [e[1] for e in plan.entries if e[0] == "gather"]
+        assert all((a == b).all() for a, b in zip(numpy_maps, c_maps))
+    np.testing.assert_allclose(plan.run(np.complex128), want, atol=1e-12)
+    np.testing.assert_allclose(plan.run(np.complex64), want, atol=2e-6)
+    obs = [("PauliZ", [i]) for i in range(n)]
+    zs = plan.expval_z(plan.run(np.complex128), cplan.z_masks(n))
+    ref = O.expval_density(want.reshape(2**n, 2**n), n, obs) if noisy else O.expval_state(want, n, obs)
+    np.testing.assert_allclose(zs, ref, atol=1e-12)

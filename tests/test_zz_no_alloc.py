@@ -4,7 +4,8 @@ under a fixed device-memory budget).  Its workspace is a static 4 MiB device
 array inside libjqsim, so the call itself allocates nothing.
 
 Checked through the C ABI against jq_forward (caller-provided workspace) on
-two calls in a row, plus its two rejections: a plan that is not yet resident
+two calls in a row, with the device's free memory unchanged across each call,
+plus its two rejections: a plan that is not yet resident
 on the device and a workspace above the static limit.  Collected last so that
 a run stopping at the first failure has already run every other test.
 """
@@ -73,9 +74,13 @@ def test_noalloc_forward_matches_forward(dtype):
     for _ in range(2):
         state.fill_(float("nan"))
         out.fill_(float("nan"))
+        torch.cuda.synchronize()
+        free_before = torch.cuda.mem_get_info()[0]
         L.check(lib.jq_forward_noalloc(plan.handle, 1, _vp(angles), None, None, 0, L.JQ_OUT_EXPVAL, _vp(state),
                                        _vp(out), stream))
         torch.cuda.synchronize()
+        # the call itself took no device memory
+        assert torch.cuda.mem_get_info()[0] == free_before
         np.testing.assert_allclose(out.cpu().numpy(), ref_out.cpu().numpy(), atol=TOL[dtype], rtol=0)
         np.testing.assert_allclose(state.cpu().numpy(), ref_state.cpu().numpy(), atol=TOL[dtype], rtol=0)
 
