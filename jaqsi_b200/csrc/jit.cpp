@@ -118,6 +118,7 @@ __device__ __forceinline__ void cp_async16(void* s, const void* g) {
 }
 __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+template <int N> __device__ __forceinline__ void cp_waitn() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 __device__ __forceinline__ u32 swz8(u32 l) { return l ^ (((l >> 4) ^ (l >> 8) ^ (l >> 12)) & 15u); }
 __device__ __forceinline__ u32 swz16(u32 l) { return l ^ (((l >> 3) ^ (l >> 6) ^ (l >> 9) ^ (l >> 12)) & 7u); }
 // Asynchronous tile load (global -> swizzled shared memory, no registers):
@@ -397,6 +398,20 @@ static SplitStage plan_split(const Schedule& s, int ri0, int rb_end, int nr, int
   return res;
 }
 
+}  // namespace
+
+// Tile buffers of a forward pass (2: double buffering; JQ_JIT_BUFS=3 or 4
+// keeps more tiles in flight per CTA).
+int jit_bufs() {
+  static const int n = [] {
+    const char* e = std::getenv("JQ_JIT_BUFS");
+    return e ? std::max(2, std::min(4, std::atoi(e))) : 2;
+  }();
+  return n;
+}
+
+namespace {
+
 // Emit the kernel of pass p (register-stage program only).
 void emit_pass(std::ostringstream& o, const jq_plan* plan, const Schedule& s, int p, bool c64, int rb) {
   const PassDesc& pd = s.passes[p];
@@ -420,11 +435,12 @@ void emit_pass(std::ostringstream& o, const jq_plan* plan, const Schedule& s, in
   o << "extern \"C\" __global__ void __launch_bounds__(" << nthr << ", " << minb << ") @KERNEL@(" << T
     << "* __restrict__ state, int batch, const " << T << "* __restrict__ bmat, long long bstride, "
     << "const int* __restrict__ mc) {\n";
-  // two tile buffers: the next tile streams in (cp.async) while this one is computed
+  // nbuf tile buffers: the next nbuf - 1 tiles stream in (cp.async) while
+  // this one is computed
+  const int nbuf = jit_bufs();
   o << "  extern __shared__ __align__(16) unsigned char smem[];\n";
   o << "  " << T << "* s0 = (" << T << "*)smem;\n";
-  o << "  " << T << "* s1 = s0 + " << (1 << t) << ";\n";
-  o << "  " << T << "* smat = s1 + " << (1 << t) << ";\n";
+  o << "  " << T << "* smat = s0 + " << nbuf * (1 << t) << ";\n";
   if (c64) {
     // broadcast copies (re, re), (im, im) of every staged matrix entry
     o << "  float2* smatb = smat + " << smat_pad << ";\n";
@@ -486,13 +502,19 @@ void emit_pass(std::ostringstream& o, const jq_plan* plan, const Schedule& s, in
   o << "  auto gaddr = [&](long long tl) { const u64 ti = (u64)tl & (u64)(tiles_per - 1); return state + ((tl >> "
     << (nb - t) << ") << " << nb << ") + " << pdep_expr("ti", outer) << "; };\n";
   o << "  __syncthreads();\n";
-  o << "  if ((long long)blockIdx.x < ntiles) " << pf << "(s0, gaddr(blockIdx.x), tbl);\n";
-  o << "  cp_commit();\n";
+  for (int j = 0; j + 1 < nbuf; ++j) {
+    o << "  if ((long long)blockIdx.x + " << j << "ll * gridDim.x < ntiles) " << pf << "(s0 + " << j * (1 << t)
+      << ", gaddr(blockIdx.x + " << j << "ll * gridDim.x), tbl);\n";
+    o << "  cp_commit();\n";
+  }
   o << "  long long last_inst = -1;\n";
-  o << "  int kk = 0;\n";
-  o << "  for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++kk) {\n";
-  o << "    " << T << "* s = (kk & 1) ? s1 : s0;\n";
-  o << "    if (tile + gridDim.x < ntiles) " << pf << "((kk & 1) ? s0 : s1, gaddr(tile + gridDim.x), tbl);\n";
+  o << "  int cur = 0;\n";
+  o << "  for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {\n";
+  o << "    " << T << "* s = s0 + cur * " << (1 << t) << ";\n";
+  o << "    { const int nx = cur == 0 ? " << nbuf - 1 << " : cur - 1;  // the buffer computed last\n";
+  o << "      const long long ahead = tile + " << nbuf - 1 << "ll * gridDim.x;\n";
+  o << "      if (ahead < ntiles) " << pf << "(s0 + nx * " << (1 << t) << ", gaddr(ahead), tbl); }\n";
+  o << "    cur = cur + 1 == " << nbuf << " ? 0 : cur + 1;\n";
   o << "    cp_commit();\n";
   o << "    const long long inst = tile >> " << (nb - t) << ";\n";
   o << "    " << T << "* g = gaddr(tile);\n";
@@ -506,7 +528,7 @@ void emit_pass(std::ostringstream& o, const jq_plan* plan, const Schedule& s, in
   else
     o << "        for (int e = tid; e < n; e += blockDim.x) smat[d + e] = bm[a + e]; }\n";
   o << "      (void)bm; last_inst = inst;\n    }\n";
-  o << "    cp_wait1();\n";
+  o << "    cp_waitn<" << nbuf - 1 << ">();\n";
   o << "    __syncthreads();\n";
   nstage = 0;
   for (int si = pd.step_begin; si < pd.step_end; ++si) {
@@ -1220,7 +1242,7 @@ void jit_free(JitModule* m) {
 size_t jit_smem(const Schedule& s, int p, int elem) {
   const PassDesc& pd = s.passes[p];
   const size_t smat_pad = static_cast<size_t>((pd.smat_len + 1) & ~1);
-  return 2 * (static_cast<size_t>(1) << pd.t) * elem + smat_pad * elem + (elem == 8 ? 2 * smat_pad * elem : 0) +
+  return jit_bufs() * (static_cast<size_t>(1) << pd.t) * elem + smat_pad * elem + (elem == 8 ? 2 * smat_pad * elem : 0) +
          (static_cast<size_t>(1) << (pd.t - pd.c)) * 4;
 }
 

@@ -28,6 +28,7 @@ bool jit_pass_eligible(const Schedule& s, int p);
 int jit_build(const jq_plan* plan, const Schedule& s, JitModule* out);
 void jit_free(JitModule* m);
 size_t jit_smem(const Schedule& s, int p, int elem);
+int jit_bufs();
 int jit_launch(const JitModule& m, const Schedule& s, int p, int n_bits, int sm_count, void* state, int batch,
                const void* bmat, int64_t bstride, int elem, cudaStream_t st);
 
