@@ -657,6 +657,21 @@ def simulate_and_measure(
     uses the checkpointed reverse pass.  ``dtype`` selects complex64 or
     complex128 (default :func:`~jaqsi_b200.operations.cdtype`).
     """
+    _check_type(type, use_density)
+    dev = _device()
+    lw = lower_tape(tape, n_qubits)
+    return execute_lowered(lw, n_qubits, type, obs, use_density, gather_angles(lw.angles, dev),
+                           gather_mats(lw.mats, dev), shots=shots, key=key, initial_state=initial_state,
+                           dtype=dtype, tune=tune)
+
+
+def execute_lowered(lw: Lowered, n_qubits: int, type: str, obs, use_density: bool, angles, mats,
+                    shots: Optional[int] = None, key=None, initial_state=None, dtype=None,
+                    tune: Optional[dict] = None, plans: Optional[dict] = None) -> torch.Tensor:
+    """Run a lowered tape with its gathered angles / matrices (device
+    tensors) and measure: the tail of simulate_and_measure.  ``plans``, when
+    given, memoises the plan per (observables, mode, dtype, tune) for a
+    caller that keeps one lowering across calls."""
     obs = list(obs or [])
     _check_type(type, use_density)
     dt = _resolve_dtype(dtype)
@@ -664,11 +679,13 @@ def simulate_and_measure(
     exact = shots is None or type not in ("probs", "expval")
     mtype = type if exact else "probs"
     mode = L.JQ_DENSITY if use_density else L.JQ_STATEVECTOR
-    lw = lower_tape(tape, n_qubits)
     specs, okey = _lower_obs(obs if mtype == "expval" else [], n_qubits)
-    plan = get_plan(lw, specs, okey, n_qubits, mode, dt, tune)
-    angles = gather_angles(lw.angles, dev)
-    mats = gather_mats(lw.mats, dev)
+    pk = (okey, n_qubits, mode, dt, tuple(sorted((tune or {}).items())))
+    plan = plans.get(pk) if plans is not None else None
+    if plan is None:
+        plan = get_plan(lw, specs, okey, n_qubits, mode, dt, tune)
+        if plans is not None:
+            plans[pk] = plan
     init, init_b = _prepare_init(initial_state, n_qubits, dt, dev, batched_ok=False)
     res = run_plan(plan, _OUT[mtype], 1, angles, mats, init, init_b)[0]
     if not exact:
