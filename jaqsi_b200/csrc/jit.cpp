@@ -1033,6 +1033,396 @@ void emit_adj_pass(std::ostringstream& o, const jq_plan* plan, const Schedule& s
   o << "  }\n  __syncthreads();\n  if (last_inst >= 0) {\n" << flush_for("last_inst") << "  }\n}\n";
 }
 
+// Forward application of register op `ro` to the registers arr<var[j]>
+// (j = register slot): the non-split forms of emit_pass.  Unguarded
+// permutations rename `var` at generation time.
+void emit_fwd_rop(std::ostringstream& o, const RegOp& ro, bool c64, const std::string& arr, std::vector<int>& var,
+                  int nr) {
+  const char* T = c64 ? "float2" : "double2";
+  const uint32_t kind = ro.w0 & 15u, q1 = (ro.w0 >> 4) & 15u, q2 = (ro.w0 >> 8) & 15u;
+  const uint32_t dk = (ro.w0 >> 12) & 15u, dq = ro.w0 >> 16;
+  const uint32_t crm = ro.w1 & 0xFFu, ctm = (ro.w1 >> 8) & 0xFFFFu, perm = ro.w1 >> 24;
+  const uint32_t M = ro.w2;
+  const bool guard = ctm != 0;
+  auto V = [&](int j) { return arr + std::to_string(var[j]); };
+  if (guard) o << "      if ((tid & " << ctm << "u) == " << ctm << "u) {\n";
+  else o << "      {\n";
+  if (kind == RK_DENSE1) {
+    if (c64) {
+      o << "        const float4* mq = (const float4*)smatb + " << M << ";\n";
+      o << "        const float4 A = mq[0], Bq = mq[1], Cq = mq[2], Dq = mq[3];\n";
+      o << "        const float2 ar = lo2(A), ai = hi2(A), br = lo2(Bq), bi = hi2(Bq), cr = lo2(Cq), ci = hi2(Cq), "
+           "dr = lo2(Dq), di = hi2(Dq);\n";
+    } else {
+      o << "        const double2 m00 = smat[" << M << "], m01 = smat[" << M + 1 << "], m10 = smat[" << M + 2
+        << "], m11 = smat[" << M + 3 << "];\n";
+    }
+    for (int j = 0; j < nr; ++j) {
+      if ((j >> q1) & 1) continue;
+      if ((static_cast<uint32_t>(j) & crm) != crm) continue;
+      const int k = j | (1 << q1);
+      if (c64)
+        o << "        { const float2 x = " << V(j) << ", y = " << V(k) << "; " << V(j) << " = cdot2(ar, ai, br, bi, x, y); "
+          << V(k) << " = cdot2(cr, ci, dr, di, x, y); }\n";
+      else
+        o << "        { const double2 x = " << V(j) << ", y = " << V(k) << "; " << V(j) << " = cfma(m01, y, cmul(m00, x)); "
+          << V(k) << " = cfma(m11, y, cmul(m10, x)); }\n";
+    }
+  } else if (kind == RK_PERM1) {
+    for (int j = 0; j < nr; ++j) {
+      if ((j >> q1) & 1) continue;
+      if ((static_cast<uint32_t>(j) & crm) != crm) continue;
+      const int k = j | (1 << q1);
+      if (!guard) std::swap(var[j], var[k]);
+      else o << "        { const " << T << " x = " << V(j) << "; " << V(j) << " = " << V(k) << "; " << V(k) << " = x; }\n";
+    }
+  } else if (kind == RK_DIAG) {
+    for (int j = 0; j < nr; ++j) {
+      if ((static_cast<uint32_t>(j) & crm) != crm) continue;
+      int idx = 0;
+      for (uint32_t i = 0; i < dk; ++i) idx = (idx << 1) | ((j >> ((dq >> (3 * i)) & 7u)) & 1);
+      o << "        " << V(j) << " = cmul(smat[" << M + idx << "], " << V(j) << ");\n";
+    }
+  } else if (kind == RK_DENSE2) {
+    for (int j = 0; j < nr; ++j) {
+      if (((j >> q1) & 1) || ((j >> q2) & 1)) continue;
+      if ((static_cast<uint32_t>(j) & crm) != crm) continue;
+      const int id[4] = {j, j | (1 << q2), j | (1 << q1), j | (1 << q1) | (1 << q2)};
+      o << "        { const " << T << " a0 = " << V(id[0]) << ", a1 = " << V(id[1]) << ", a2 = " << V(id[2])
+        << ", a3 = " << V(id[3]) << ";\n";
+      for (int r = 0; r < 4; ++r) {
+        if (c64)
+          o << "          " << V(id[r]) << " = cdot4((const float4*)smatb + " << M + 4 * r << ", a0, a1, a2, a3);\n";
+        else
+          o << "          " << V(id[r]) << " = cfma(smat[" << M + 4 * r + 3 << "], a3, cfma(smat[" << M + 4 * r + 2
+            << "], a2, cfma(smat[" << M + 4 * r + 1 << "], a1, cmul(smat[" << M + 4 * r << "], a0))));\n";
+      }
+      o << "        }\n";
+    }
+  } else {  // RK_PERM2: output row r takes input column p[r]
+    for (int j = 0; j < nr; ++j) {
+      if (((j >> q1) & 1) || ((j >> q2) & 1)) continue;
+      if ((static_cast<uint32_t>(j) & crm) != crm) continue;
+      const int id[4] = {j, j | (1 << q2), j | (1 << q1), j | (1 << q1) | (1 << q2)};
+      int pv[4];
+      for (int r = 0; r < 4; ++r) pv[r] = (perm >> (2 * r)) & 3u;
+      if (!guard) {
+        int nv[4];
+        for (int r = 0; r < 4; ++r) nv[r] = var[id[pv[r]]];
+        for (int r = 0; r < 4; ++r) var[id[r]] = nv[r];
+      } else {
+        o << "        { const " << T << " a0 = " << V(id[0]) << ", a1 = " << V(id[1]) << ", a2 = " << V(id[2])
+          << ", a3 = " << V(id[3]) << ";";
+        for (int r = 0; r < 4; ++r) o << " " << V(id[r]) << " = a" << pv[r] << ";";
+        o << " }\n";
+      }
+    }
+  }
+  o << "      }\n";
+}
+
+// Shared memory of a checkpointed reverse pass: the input tile of every
+// register stage, the lambda tile, staged matrices, float64 cotangent
+// accumulators and the bit-deposit table.
+size_t bwd_smem_bytes(const Schedule& s, int p, int elem) {
+  const PassDesc& pd = s.passes[p];
+  int nacc = 0;
+  for (int ri = pd.rop_begin; ri < pd.rop_end; ++ri)
+    if (s.rops[ri].grad_off >= 0) nacc += 2 * s.rops[ri].mat_len;
+  const size_t smat_pad = static_cast<size_t>((pd.smat_len + 1) & ~1);
+  const size_t nst = static_cast<size_t>(pd.step_end - pd.step_begin);
+  return (nst + 1) * (static_cast<size_t>(1) << pd.t) * elem + smat_pad * elem + (elem == 8 ? 2 * smat_pad * elem : 0) +
+         static_cast<size_t>((nacc + 1) & ~1) * 8 + (static_cast<size_t>(1) << (pd.t - pd.c)) * 4;
+}
+
+// Emit the checkpointed reverse kernel of pass p (density matrices with
+// channels, non-unitary pure circuits).  Per tile: the pass input x and the
+// cotangent lam after the pass are loaded; a forward walk runs the register
+// stages, each writing its output into a fresh shared-memory tile, so the
+// input of every stage is kept; then the stages run in reverse.  Inside a
+// stage the state before each gate block is recomputed in registers from the
+// stage input (the stage's earlier blocks, a handful), the block cotangent
+// lam x^dagger is accumulated (warp reduce-scatter into float64 shared
+// accumulators, flushed per instance) and lam <- G^dagger lam.  Unguarded
+// permutations stay register renames in both directions.
+void emit_bwd_pass(std::ostringstream& o, const jq_plan* plan, const Schedule& s, int p, bool c64, int rb) {
+  const PassDesc& pd = s.passes[p];
+  const char* T = c64 ? "float2" : "double2";
+  const char* F = c64 ? "float" : "double";
+  const int t = pd.t, c = pd.c, nb = plan->n_bits;
+  const int nthr = 1 << (t - rb);
+  const int nr = 1 << rb;
+  const int nst = pd.step_end - pd.step_begin;
+  const uint64_t full = (nb >= 64) ? ~0ULL : ((1ULL << nb) - 1);
+  const uint64_t outer = full & ~pd.tile_mask;
+  const int smat_pad = (pd.smat_len + 1) & ~1;
+  int nmc = 0, ngt = 0, nacc = 0;
+  std::vector<int> acc_off(pd.rop_end - pd.rop_begin, -1);
+  for (int ri = pd.rop_begin; ri < pd.rop_end; ++ri) {
+    const RegOp& ro = s.rops[ri];
+    nmc += ro.mat_len > 0;
+    if (ro.grad_off >= 0) {
+      acc_off[ri - pd.rop_begin] = nacc;
+      nacc += 2 * ro.mat_len;
+      ++ngt;
+    }
+  }
+  const int nacc_pad = (nacc + 1) & ~1;
+  o << "extern \"C\" __global__ void __launch_bounds__(" << nthr << ", 1) @KERNEL@(" << T
+    << "* __restrict__ xin, " << T << "* __restrict__ lam, int batch, const " << T
+    << "* __restrict__ bmat, long long bstride, const int* __restrict__ mc, double* __restrict__ gacc, "
+    << "long long gstride, const int* __restrict__ gt) {\n";
+  o << "  extern __shared__ __align__(16) unsigned char smem[];\n";
+  o << "  " << T << "* sx = (" << T << "*)smem;  // stage inputs, " << nst << " tiles\n";
+  o << "  " << T << "* sl = sx + " << nst * (1 << t) << ";\n";
+  o << "  " << T << "* smat = sl + " << (1 << t) << ";\n";
+  if (c64) {
+    o << "  float2* smatb = smat + " << smat_pad << ";\n";
+    o << "  double* sacc = (double*)(smatb + " << 2 * smat_pad << ");\n";
+  } else {
+    o << "  double* sacc = (double*)(smat + " << smat_pad << ");\n";
+  }
+  o << "  u32* tbl = (u32*)(sacc + " << nacc_pad << ");\n";
+  o << "  const u32 tid = threadIdx.x;\n";
+  o << "  { const u32 hb[] = {";
+  for (int i = c; i < t; ++i) o << (i > c ? ", " : "") << (1u << pd.bits[i]);
+  if (t == c) o << "0u";
+  o << "};\n    for (int h = tid; h < " << (1 << (t - c)) << "; h += blockDim.x) { u32 v = 0;";
+  o << " for (int i = 0; i < " << (t - c) << "; ++i) if ((h >> i) & 1) v |= hb[i]; tbl[h] = v; } }\n";
+  o << "  for (int e = tid; e < " << nacc_pad << "; e += blockDim.x) sacc[e] = 0.0;\n";
+  std::vector<std::vector<uint32_t>> offs(nst);
+  for (int k = 0; k < nst; ++k) {
+    const Step& st = s.steps[pd.step_begin + k];
+    o << "  u32 tb" << k << " = 0;";
+    for (int i = 0; i < t - rb; ++i) o << " if (tid & " << (1u << i) << "u) tb" << k << " ^= " << st.tbits[i] << "u;";
+    o << "\n";
+    offs[k].resize(nr);
+    for (int j = 0; j < nr; ++j) {
+      uint32_t a = 0;
+      for (int q = 0; q < rb; ++q)
+        if ((j >> q) & 1) a ^= st.ebits[q];
+      offs[k][j] = a;
+    }
+  }
+  // lambda leaves the last reverse stage (the pass's first) straight to
+  // global memory under the forward pass's direct-store condition
+  const Step& fin = s.steps[pd.step_begin];
+  bool direct = t - rb >= 2 && c >= 2 && (c64 ? (fin.tbits[0] == 1u && fin.tbits[1] == 2u) : fin.tbits[0] == 1u);
+  if (const char* e = std::getenv("JQ_JIT_DIRECT_STORE")) direct = direct && std::atoi(e) != 0;
+  const bool wide = nb > 31;
+  auto unswz = [&](uint64_t v) -> uint64_t {
+    if (c64) return v ^ (((v >> 4) ^ (v >> 8) ^ (v >> 12)) & 15u);
+    return v ^ (((v >> 3) ^ (v >> 6) ^ (v >> 9) ^ (v >> 12)) & 7u);
+  };
+  auto gdep = [&](uint64_t logical) -> uint64_t {
+    uint64_t g = 0;
+    for (int i = 0; i < t; ++i)
+      if ((logical >> i) & 1) g |= 1ULL << pd.bits[i];
+    return g;
+  };
+  if (direct) {
+    o << "  " << (wide ? "u64" : "u32") << " gpos = 0;";
+    for (int i = 0; i < t - rb; ++i)
+      o << " if (tid & " << (1u << i) << "u) gpos ^= " << gdep(unswz(fin.tbits[i])) << (wide ? "ull;" : "u;");
+    o << "\n";
+  }
+  auto flush_for = [&](const std::string& inst) {
+    return "      if (gacc) for (int i = 0; i < " + std::to_string(ngt) +
+           "; ++i) { const int so = gt[3 * i], go = gt[3 * i + 1], n = gt[3 * i + 2];\n"
+           "        for (int e = tid; e < n; e += blockDim.x) atomicAdd(&gacc[" + inst +
+           " * gstride * 2 + 2 * go + e], sacc[so + e]); }\n";
+  };
+  o << "  const long long tiles_per = 1ll << " << (nb - t) << ";\n";
+  o << "  const long long ntiles = tiles_per * batch;\n";
+  o << "  long long last_inst = -1;\n";
+  o << "  for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {\n";
+  o << "    const long long inst = tile >> " << (nb - t) << ";\n";
+  o << "    const u64 ti = (u64)tile & (u64)(tiles_per - 1);\n";
+  o << "    const long long goff = (inst << " << nb << ") + (long long)" << pdep_expr("ti", outer) << ";\n";
+  o << "    __syncthreads();\n";
+  o << "    if (inst != last_inst) {\n";
+  o << "      if (last_inst >= 0) {\n" << flush_for("last_inst") << "        __syncthreads();\n";
+  o << "        for (int e = tid; e < " << nacc_pad << "; e += blockDim.x) sacc[e] = 0.0;\n      }\n";
+  o << "      const " << T << "* bm = bmat + inst * bstride;\n";
+  o << "      for (int i = 0; i < " << nmc << "; ++i) { const int d = mc[3 * i], a = mc[3 * i + 1], n = mc[3 * i + 2];\n";
+  if (c64)
+    o << "        for (int e = tid; e < n; e += blockDim.x) { const float2 v = bm[a + e]; smat[d + e] = v; "
+         "smatb[2 * (d + e)] = make_float2(v.x, v.x); smatb[2 * (d + e) + 1] = make_float2(v.y, v.y); } }\n";
+  else
+    o << "        for (int e = tid; e < n; e += blockDim.x) smat[d + e] = bm[a + e]; }\n";
+  o << "      (void)bm; last_inst = inst;\n      __syncthreads();\n    }\n";
+  const std::string tpl = "<" + std::to_string(t - rb) + ", " + std::to_string(t) + ", " + std::to_string(c) + ">";
+  o << "    " << (c64 ? "prefetch8t" : "prefetch16t") << tpl << "(sx, xin + goff, tbl);\n";
+  o << "    " << (c64 ? "prefetch8t" : "prefetch16t") << tpl << "(sl, lam + goff, tbl);\n";
+  o << "    cp_commit();\n    cp_wait0();\n";
+  o << "    __syncthreads();\n";
+  // forward walk: stage k reads tile k and writes tile k + 1
+  for (int k = 0; k + 1 < nst; ++k) {
+    const Step& st = s.steps[pd.step_begin + k];
+    std::vector<int> var(nr);
+    for (int j = 0; j < nr; ++j) var[j] = j;
+    o << "    {\n      const " << T << "* src = sx + " << k * (1 << t) << ";\n      " << T << "* dst = sx + "
+      << (k + 1) * (1 << t) << ";\n";
+    for (int j = 0; j < nr; ++j) o << "      " << T << " v" << j << " = src[tb" << k << " ^ " << offs[k][j] << "u];\n";
+    for (int ri = st.a; ri < st.b; ++ri) emit_fwd_rop(o, s.rops[ri], c64, "v", var, nr);
+    for (int j = 0; j < nr; ++j) o << "      dst[tb" << k << " ^ " << offs[k][j] << "u] = v" << var[j] << ";\n";
+    o << "    }\n    __syncthreads();\n";
+  }
+  // reverse walk over the stages
+  for (int k = nst - 1; k >= 0; --k) {
+    const Step& st = s.steps[pd.step_begin + k];
+    std::vector<int> lvar(nr);
+    for (int j = 0; j < nr; ++j) lvar[j] = j;
+    o << "    {\n      const " << T << "* src = sx + " << k * (1 << t) << ";\n";
+    for (int j = 0; j < nr; ++j) o << "      " << T << " l" << j << " = sl[tb" << k << " ^ " << offs[k][j] << "u];\n";
+    for (int ri = st.b - 1; ri >= st.a; --ri) {
+      const RegOp& ro = s.rops[ri];
+      const uint32_t kind = ro.w0 & 15u, q1 = (ro.w0 >> 4) & 15u, q2 = (ro.w0 >> 8) & 15u;
+      const uint32_t dk = (ro.w0 >> 12) & 15u, dq = ro.w0 >> 16;
+      const uint32_t crm = ro.w1 & 0xFFu, ctm = (ro.w1 >> 8) & 0xFFFFu, perm = ro.w1 >> 24;
+      const uint32_t M = ro.w2;
+      const bool guard = ctm != 0;
+      const bool grad = ro.grad_off >= 0;
+      const int ao = acc_off[ri - pd.rop_begin];
+      auto Lm = [&](int j) { return std::string("l") + std::to_string(lvar[j]); };
+      if (kind == RK_PERM1 || kind == RK_PERM2) {
+        // lam <- P^-1 lam: renames, or explicit moves under a thread-bit control
+        if (guard) o << "      if ((tid & " << ctm << "u) == " << ctm << "u) {\n";
+        for (int j = 0; j < nr; ++j) {
+          if (kind == RK_PERM1) {
+            if ((j >> q1) & 1) continue;
+            if ((static_cast<uint32_t>(j) & crm) != crm) continue;
+            const int kk = j | (1 << q1);
+            if (!guard) std::swap(lvar[j], lvar[kk]);
+            else o << "        { const " << T << " x = " << Lm(j) << "; " << Lm(j) << " = " << Lm(kk) << "; " << Lm(kk) << " = x; }\n";
+          } else {
+            if (((j >> q1) & 1) || ((j >> q2) & 1)) continue;
+            if ((static_cast<uint32_t>(j) & crm) != crm) continue;
+            const int id[4] = {j, j | (1 << q2), j | (1 << q1), j | (1 << q1) | (1 << q2)};
+            int pv[4];
+            for (int r = 0; r < 4; ++r) pv[r] = (perm >> (2 * r)) & 3u;
+            if (!guard) {
+              int nv[4];
+              for (int r = 0; r < 4; ++r) nv[pv[r]] = lvar[id[r]];
+              for (int r = 0; r < 4; ++r) lvar[id[r]] = nv[r];
+            } else {
+              o << "        { const " << T << " a0 = " << Lm(id[0]) << ", a1 = " << Lm(id[1]) << ", a2 = " << Lm(id[2])
+                << ", a3 = " << Lm(id[3]) << ";";
+              for (int r = 0; r < 4; ++r) o << " " << Lm(id[pv[r]]) << " = a" << r << ";";
+              o << " }\n";
+            }
+          }
+        }
+        if (guard) o << "      }\n";
+        continue;
+      }
+      // the state before this block: the stage input with the stage's
+      // earlier blocks applied (registers y*)
+      std::vector<int> yvar(nr);
+      for (int j = 0; j < nr; ++j) yvar[j] = j;
+      o << "      {\n";
+      for (int j = 0; j < nr; ++j) o << "      " << T << " y" << j << " = src[tb" << k << " ^ " << offs[k][j] << "u];\n";
+      for (int rj = st.a; rj < ri; ++rj) emit_fwd_rop(o, s.rops[rj], c64, "y", yvar, nr);
+      auto Y = [&](int j) { return std::string("y") + std::to_string(yvar[j]); };
+      int ng = 0;
+      if (grad) {
+        ng = (kind == RK_DIAG) ? (1 << dk) : (kind == RK_DENSE1 ? 4 : 16);
+        o << "        " << T << " g[" << ng << "];\n        for (int e = 0; e < " << ng
+          << "; ++e) { g[e].x = 0; g[e].y = 0; }\n";
+      }
+      if (guard) o << "        if ((tid & " << ctm << "u) == " << ctm << "u) {\n";
+      else o << "        {\n";
+      if (kind == RK_DENSE1) {
+        if (c64)
+          o << "          const float4* mq = (const float4*)smatb + " << M << ";\n"
+            << "          const float4 A = mq[0], Bq = mq[2], Cq = mq[1], Dq = mq[3];\n"
+            << "          const float2 ar = lo2(A), ai = hi2(A), br = lo2(Bq), bi = hi2(Bq), cr = lo2(Cq), ci = hi2(Cq), "
+               "dr = lo2(Dq), di = hi2(Dq);\n";
+        else
+          o << "          const double2 h00 = cconj(smat[" << M << "]), h01 = cconj(smat[" << M + 2
+            << "]), h10 = cconj(smat[" << M + 1 << "]), h11 = cconj(smat[" << M + 3 << "]);\n";
+        for (int j = 0; j < nr; ++j) {
+          if ((j >> q1) & 1) continue;
+          if ((static_cast<uint32_t>(j) & crm) != crm) continue;
+          const int kk = j | (1 << q1);
+          if (grad)
+            o << "          g[0] = cadd(g[0], cmulc(" << Lm(j) << ", " << Y(j) << ")); g[1] = cadd(g[1], cmulc(" << Lm(j)
+              << ", " << Y(kk) << ")); g[2] = cadd(g[2], cmulc(" << Lm(kk) << ", " << Y(j)
+              << ")); g[3] = cadd(g[3], cmulc(" << Lm(kk) << ", " << Y(kk) << "));\n";
+          if (c64)
+            o << "          { const float2 x = " << Lm(j) << ", y = " << Lm(kk) << "; " << Lm(j)
+              << " = cdot2c(ar, ai, br, bi, x, y); " << Lm(kk) << " = cdot2c(cr, ci, dr, di, x, y); }\n";
+          else
+            o << "          { const double2 x = " << Lm(j) << ", y = " << Lm(kk) << "; " << Lm(j)
+              << " = cfma(h01, y, cmul(h00, x)); " << Lm(kk) << " = cfma(h11, y, cmul(h10, x)); }\n";
+        }
+      } else if (kind == RK_DIAG) {
+        for (int j = 0; j < nr; ++j) {
+          if ((static_cast<uint32_t>(j) & crm) != crm) continue;
+          int idx = 0;
+          for (uint32_t i = 0; i < dk; ++i) idx = (idx << 1) | ((j >> ((dq >> (3 * i)) & 7u)) & 1);
+          o << "          {";
+          if (grad) o << " g[" << idx << "] = cadd(g[" << idx << "], cmulc(" << Lm(j) << ", " << Y(j) << "));";
+          o << " " << Lm(j) << " = cmul(cconj(smat[" << M + idx << "]), " << Lm(j) << "); }\n";
+        }
+      } else {  // RK_DENSE2
+        auto B = [&](uint32_t e, int part) { return "smatb[" + std::to_string(2 * (M + e) + part) + "]"; };
+        auto H = [&](int r, int q) { return "cconj(smat[" + std::to_string(M + 4 * q + r) + "])"; };
+        auto HC = [&](const std::string& dst, int r) {
+          std::string e = "{ float2 p = __fmul2_rn(" + B(r, 0) + ", b0), q = __fmul2_rn(" + B(r, 1) + ", b0);";
+          for (int q = 1; q < 4; ++q)
+            e += " p = __ffma2_rn(" + B(4 * q + r, 0) + ", b" + std::to_string(q) + ", p); q = __ffma2_rn(" +
+                 B(4 * q + r, 1) + ", b" + std::to_string(q) + ", q);";
+          return e + " " + dst + " = make_float2(p.x + q.y, p.y - q.x); }";
+        };
+        for (int j = 0; j < nr; ++j) {
+          if (((j >> q1) & 1) || ((j >> q2) & 1)) continue;
+          if ((static_cast<uint32_t>(j) & crm) != crm) continue;
+          const int id[4] = {j, j | (1 << q2), j | (1 << q1), j | (1 << q1) | (1 << q2)};
+          o << "          {\n";
+          if (grad)
+            for (int r = 0; r < 4; ++r)
+              for (int q = 0; q < 4; ++q)
+                o << "            g[" << 4 * r + q << "] = cadd(g[" << 4 * r + q << "], cmulc(" << Lm(id[r]) << ", "
+                  << Y(id[q]) << "));\n";
+          o << "            const " << T << " b0 = " << Lm(id[0]) << ", b1 = " << Lm(id[1]) << ", b2 = " << Lm(id[2])
+            << ", b3 = " << Lm(id[3]) << ";\n";
+          for (int r = 0; r < 4; ++r) {
+            if (c64) o << "            " << HC(Lm(id[r]), r) << "\n";
+            else
+              o << "            " << Lm(id[r]) << " = cfma(" << H(r, 3) << ", b3, cfma(" << H(r, 2) << ", b2, cfma("
+                << H(r, 1) << ", b1, cmul(" << H(r, 0) << ", b0))));\n";
+          }
+          o << "          }\n";
+        }
+      }
+      o << "        }\n";
+      if (grad) {
+        const int nv = 2 * ng;
+        for (int c0 = 0; c0 < nv; c0 += 32) {
+          const int cn = std::min(32, nv - c0);
+          o << "        { " << F << " vv[" << cn << "] = {";
+          for (int e = 0; e < cn; ++e)
+            o << (e ? ", " : "") << "g[" << (c0 + e) / 2 << "]." << (((c0 + e) & 1) ? "y" : "x");
+          o << "}; warp_rs_add<" << cn << ">(vv, &sacc[" << ao + c0 << "]); }\n";
+        }
+      }
+      o << "      }\n";
+    }
+    if (direct && k == 0) {
+      for (int j = 0; j < nr; ++j)
+        o << "      __stcs(lam + goff + (gpos ^ " << gdep(unswz(offs[k][j])) << (wide ? "ull" : "u") << "), l"
+          << lvar[j] << ");\n";
+      o << "    }\n";
+    } else {
+      for (int j = 0; j < nr; ++j) o << "      sl[tb" << k << " ^ " << offs[k][j] << "u] = l" << lvar[j] << ";\n";
+      o << "    }\n    __syncthreads();\n";
+    }
+  }
+  if (!direct) o << "    " << (c64 ? "store8t" : "store16t") << tpl << "(sl, lam + goff, tbl);\n";
+  o << "  }\n  __syncthreads();\n  if (last_inst >= 0) {\n" << flush_for("last_inst") << "  }\n}\n";
+}
+
 }  // namespace
 
 bool jit_available() {
@@ -1050,15 +1440,21 @@ bool jit_pass_eligible(const Schedule& s, int p) {
 
 // Kernel text of every eligible pass (forward, or adjoint when `adjoint`);
 // identical texts share one kernel.  Appends to `all`, names kernels prefix + k.
-void emit_kernels(const jq_plan* plan, const Schedule& s, bool adjoint, const char* prefix, std::ostringstream& all,
+// mode 0: forward passes, 1: adjoint passes (unitary statevector plans),
+// 2: checkpointed reverse passes (every other plan; passes whose stage inputs
+// do not fit in shared memory keep the generic kernel).
+void emit_kernels(const jq_plan* plan, const Schedule& s, int mode, const char* prefix, std::ostringstream& all,
                   std::vector<int>* kernel_of, std::vector<std::string>* names,
                   std::vector<std::string>* bodies = nullptr) {
   kernel_of->assign(s.passes.size(), -1);
   std::vector<std::string> texts;
+  const int elem = plan->dtype == JQ_C64 ? 8 : 16;
   for (int p = 0; p < static_cast<int>(s.passes.size()); ++p) {
     if (!jit_pass_eligible(s, p)) continue;
+    if (mode == 2 && bwd_smem_bytes(s, p, elem) > 227 * 1024) continue;
     std::ostringstream o;
-    if (adjoint) emit_adj_pass(o, plan, s, p, plan->dtype == JQ_C64, s.reg_bits);
+    if (mode == 1) emit_adj_pass(o, plan, s, p, plan->dtype == JQ_C64, s.reg_bits);
+    else if (mode == 2) emit_bwd_pass(o, plan, s, p, plan->dtype == JQ_C64, s.reg_bits);
     else emit_pass(o, plan, s, p, plan->dtype == JQ_C64, s.reg_bits);
     const std::string text = o.str();
     int k = -1;
@@ -1081,14 +1477,18 @@ void emit_kernels(const jq_plan* plan, const Schedule& s, bool adjoint, const ch
 // The adjoint kernels are specialised too when the plan can run jq_adjoint
 // (a unitary statevector plan).
 bool plan_wants_adjoint(const jq_plan* plan) { return plan->mode == JQ_STATEVECTOR && plan->unitary; }
+// The checkpointed reverse passes are specialised for every other plan that
+// has parameters to differentiate.
+bool plan_wants_backward(const jq_plan* plan) { return !plan_wants_adjoint(plan) && plan->any_grad; }
 
 std::string jit_source(const jq_plan* plan, const Schedule& s) {
   std::ostringstream all;
   all << kPrelude;
   std::vector<int> kernel_of;
   std::vector<std::string> names;
-  emit_kernels(plan, s, false, "jqk", all, &kernel_of, &names);
-  if (plan_wants_adjoint(plan)) emit_kernels(plan, s, true, "jqa", all, &kernel_of, &names);
+  emit_kernels(plan, s, 0, "jqk", all, &kernel_of, &names);
+  if (plan_wants_adjoint(plan)) emit_kernels(plan, s, 1, "jqa", all, &kernel_of, &names);
+  if (plan_wants_backward(plan)) emit_kernels(plan, s, 2, "jqb", all, &kernel_of, &names);
   return all.str();
 }
 
@@ -1098,13 +1498,16 @@ int jit_build(const jq_plan* plan, const Schedule& s, JitModule* out) {
     return JQ_EUNSUPPORTED;
   }
   std::ostringstream all;
-  std::vector<int> kernel_of, akernel_of;
-  std::vector<std::string> names, anames, bodies;
-  emit_kernels(plan, s, false, "jqk", all, &kernel_of, &names, &bodies);
+  std::vector<int> kernel_of, akernel_of, bkernel_of;
+  std::vector<std::string> names, anames, bnames, bodies;
+  emit_kernels(plan, s, 0, "jqk", all, &kernel_of, &names, &bodies);
   const bool adj = plan_wants_adjoint(plan);
-  if (adj) emit_kernels(plan, s, true, "jqa", all, &akernel_of, &anames, &bodies);
+  if (adj) emit_kernels(plan, s, 1, "jqa", all, &akernel_of, &anames, &bodies);
+  const bool bwd = plan_wants_backward(plan);
+  if (bwd) emit_kernels(plan, s, 2, "jqb", all, &bkernel_of, &bnames, &bodies);
   out->fn.assign(s.passes.size(), nullptr);
   out->afn.assign(s.passes.size(), nullptr);
+  out->bfn.assign(s.passes.size(), nullptr);
   out->modules.clear();
   out->mc = nullptr;
   out->gt = nullptr;
@@ -1182,8 +1585,10 @@ int jit_build(const jq_plan* plan, const Schedule& s, JitModule* out) {
     }
     return JQ_OK;
   };
-  std::vector<void*> fk, ak;
-  if (lookup(names, 0, &fk) || lookup(anames, static_cast<int>(names.size()), &ak)) return JQ_ECUDA;
+  std::vector<void*> fk, ak, bk;
+  if (lookup(names, 0, &fk) || lookup(anames, static_cast<int>(names.size()), &ak) ||
+      lookup(bnames, static_cast<int>(names.size() + anames.size()), &bk))
+    return JQ_ECUDA;
   // per-pass matrix staging tables
   std::vector<int32_t> mc;
   // per-pass gradient flush tables: (shared accumulator offset, block
@@ -1193,6 +1598,7 @@ int jit_build(const jq_plan* plan, const Schedule& s, JitModule* out) {
     if (kernel_of[p] < 0) continue;
     out->fn[p] = fk[kernel_of[p]];
     if (adj && akernel_of[p] >= 0) out->afn[p] = ak[akernel_of[p]];
+    if (bwd && bkernel_of[p] >= 0) out->bfn[p] = bk[bkernel_of[p]];
     out->mc_off[p] = static_cast<int64_t>(mc.size());
     out->gt_off[p] = static_cast<int64_t>(gt.size());
     const PassDesc& pd = s.passes[p];
@@ -1221,6 +1627,7 @@ int jit_build(const jq_plan* plan, const Schedule& s, JitModule* out) {
     return JQ_ECUDA;
   }
   out->has_adjoint = adj && !anames.empty();
+  out->has_backward = bwd && !bnames.empty();
   out->n_kernels = static_cast<int>(names.size());
   return JQ_OK;
 }
@@ -1234,6 +1641,7 @@ void jit_free(JitModule* m) {
     m->mc = nullptr;
     m->gt = nullptr;
     m->afn.clear();
+    m->bfn.clear();
     m->modules.clear();
     m->fn.clear();
   }
@@ -1303,6 +1711,32 @@ int jit_launch_adj(const JitModule& m, const Schedule& s, int p, int n_bits, int
   if (g_drv.launch(f, grid, 1, 1, threads, 1, 1, static_cast<unsigned>(smem), reinterpret_cast<CUstream>(st), args,
                    nullptr) != CUDA_SUCCESS) {
     set_error("cuLaunchKernel failed for a specialised adjoint pass");
+    return JQ_ECUDA;
+  }
+  return JQ_OK;
+}
+
+int jit_launch_bwd(const JitModule& m, const Schedule& s, int p, int n_bits, int sm_count, const void* xin, void* lam,
+                   int batch, const void* bmat, int64_t bstride, double* gacc, int64_t gstride, int elem,
+                   cudaStream_t st) {
+  CUfunction f = static_cast<CUfunction>(m.bfn[p]);
+  const PassDesc& pd = s.passes[p];
+  const int threads = 1 << (pd.t - s.reg_bits);
+  const size_t smem = bwd_smem_bytes(s, p, elem);
+  int per_sm = 0;
+  g_drv.occupancy(&per_sm, f, threads, smem);
+  if (per_sm < 1) per_sm = 1;
+  const int64_t ntiles = (1LL << (n_bits - pd.t)) * batch;
+  const int64_t cap = static_cast<int64_t>(sm_count) * per_sm;
+  const unsigned grid = static_cast<unsigned>(std::max<int64_t>(1, std::min(ntiles, cap)));
+  long long bs = bstride, gs = gstride;
+  const int32_t* mc = static_cast<const int32_t*>(m.mc) + m.mc_off[p];
+  const int32_t* gt = static_cast<const int32_t*>(m.gt) + m.gt_off[p];
+  void* xp = const_cast<void*>(xin);
+  void* args[] = {&xp, &lam, &batch, const_cast<void**>(&bmat), &bs, &mc, &gacc, &gs, &gt};
+  if (g_drv.launch(f, grid, 1, 1, threads, 1, 1, static_cast<unsigned>(smem), reinterpret_cast<CUstream>(st), args,
+                   nullptr) != CUDA_SUCCESS) {
+    set_error("cuLaunchKernel failed for a specialised reverse pass");
     return JQ_ECUDA;
   }
   return JQ_OK;

@@ -78,6 +78,7 @@ struct TileOp {
   uint32_t lowmask[kMaxBlockWires];  // (1 << f) - 1 for each fixed bit f, ascending
   uint32_t tmask[kMaxBlockWires];    // 1 << target bit; tmask[0] = most significant matrix bit
   int32_t mat_off, perm_off, grad_off;
+  int32_t inv;         // 1: the block is unitary (its dagger undoes it exactly)
 };
 
 // One HBM pass: a tile covers the bits of `tile_mask`.

@@ -34,6 +34,7 @@ namespace jq {
 namespace {
 
 constexpr int kRedSlots = 64;  // doubles per warp in the block-reduction scratch
+constexpr int kMaxBwdSlots = 32;  // snapshot tiles of the checkpointed reverse pass
 
 // ---------------------------------------------------------------------------
 // index helpers
@@ -1070,39 +1071,152 @@ __device__ void bwd_diag(const C* sx, C* sl, int t, const TileOp& op, const C* _
   }
 }
 
+// Warp reduce-scatter of N (power of two, <= 32) per-lane float64 partial
+// sums by recursive halving: at the step exchanging with lane ^ O the lanes
+// with bit O set keep the upper half of the remaining values.  N - 1 shuffles
+// for the halving steps plus one per remaining lane bit; afterwards the lanes
+// whose low 5 - log2(N) bits are zero hold value lane >> (5 - log2 N), summed
+// over the warp.
+template <int O, int N>
+struct WarpRSum {
+  static __device__ __forceinline__ void run(double* v, unsigned lane) {
+    if constexpr (N > 1) {
+      constexpr int h = N / 2;
+      const bool up = (lane & O) != 0;
+#pragma unroll
+      for (int i = 0; i < h; ++i) {
+        const double send = up ? v[i] : v[i + h];
+        const double keep = up ? v[i + h] : v[i];
+        v[i] = keep + __shfl_xor_sync(0xffffffffu, send, O);
+      }
+      if constexpr (O > 1) WarpRSum<O / 2, h>::run(v, lane);
+    } else {
+      v[0] += __shfl_xor_sync(0xffffffffu, v[0], O);
+      if constexpr (O > 1) WarpRSum<O / 2, 1>::run(v, lane);
+    }
+  }
+};
+
+// Checkpointed reverse step of one dense block on k = KT bits: x is the
+// block's input (kept), lam is pulled back through G (lam <- G^dagger lam)
+// and the block cotangent lam x^dagger is added into `stage` (float64, per
+// CTA, flushed by the caller): per-lane partial sums, one warp
+// reduce-scatter, one shared atomic add per lane that holds a result.
+template <typename C, int KT>
+__device__ void bwd_dense_rs(const C* sx, C* sl, int t, const TileOp& op, const C* __restrict__ M, double* stage) {
+  constexpr int D = 1 << KT;
+  constexpr int NV = 2 * D * D;  // 8 or 32 doubles
+  const int G = 1 << (t - op.nfix);
+  const bool grad = op.grad_off >= 0 && stage != nullptr;
+  int off[D];
+#pragma unroll
+  for (int j = 0; j < D; ++j) off[j] = target_off(j, op, KT);
+  double acc[NV];
+#pragma unroll
+  for (int e = 0; e < NV; ++e) acc[e] = 0.0;
+  for (int g = threadIdx.x; g < G; g += blockDim.x) {
+    const int base = group_base(g, op);
+    C vx[D], vl[D];
+#pragma unroll
+    for (int j = 0; j < D; ++j) {
+      vx[j] = sx[base + off[j]];
+      vl[j] = sl[base + off[j]];
+    }
+    if (grad) {
+#pragma unroll
+      for (int i = 0; i < D; ++i)
+#pragma unroll
+        for (int j = 0; j < D; ++j) {
+          const double2 p = cfma(to_d2(vl[i]), cconj(to_d2(vx[j])), make_double2(acc[2 * (i * D + j)],
+                                                                                acc[2 * (i * D + j) + 1]));
+          acc[2 * (i * D + j)] = p.x;
+          acc[2 * (i * D + j) + 1] = p.y;
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < D; ++i) {
+      C a = cmake<C>(0, 0);
+#pragma unroll
+      for (int j = 0; j < D; ++j) a = cfma(cconj(__ldg(&M[j * D + i])), vl[j], a);
+      sl[base + off[i]] = a;
+    }
+  }
+  if (grad) {
+    const unsigned lane = threadIdx.x & 31u;
+    WarpRSum<16, NV>::run(acc, lane);
+    constexpr int lg = NV >= 32 ? 5 : (NV >= 16 ? 4 : 3);
+    if ((lane & ((32u >> lg) - 1u)) == 0) atomicAdd(stage + (lane >> (5 - lg)), acc[0]);
+  }
+}
+
+// Checkpointed reverse pass over one forward pass (density matrices with
+// channels, non-unitary pure circuits).  Per tile: x is the state before the
+// pass, lam the cotangent after it.  The states before the pass's blocks are
+// rebuilt in shared memory without the quadratic recompute:
+//  - a forward walk through the pass keeps snapshots of the state before
+//    each non-unitary block (slot 0 is the pass input), as many as the
+//    shared-memory budget allows (`nslot` tiles);
+//  - the reverse walk holds the state before the current block in a work
+//    tile; stepping back over a unitary block (a gate, CX halves, two-sided
+//    gates) applies its dagger, which undoes it exactly; stepping back over a
+//    non-unitary block copies its snapshot, or, for blocks beyond the
+//    snapshot budget, re-applies the blocks since the nearest earlier one.
+// Block cotangents of 1- and 2-bit dense blocks are staged per CTA (32
+// doubles per block) and flushed into the instance's accumulator when the
+// CTA moves to another instance.
 template <typename R>
 __global__ void __launch_bounds__(512, 1) k_tile_bwd(const typename CplxT<R>::T* __restrict__ x,
                                                    typename CplxT<R>::T* __restrict__ lam, int nb, int batch,
                                                    PassDesc pd, const TileOp* __restrict__ ops,
                                                    const typename CplxT<R>::T* __restrict__ bmat, int64_t bmat_stride,
-                                                   const int* __restrict__ perms, double2* gacc, int64_t grad_stride) {
+                                                   const int* __restrict__ perms, double2* gacc, int64_t grad_stride,
+                                                   int nslot) {
   using C = typename CplxT<R>::T;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int t = pd.t, c = pd.c;
-  C* sx = reinterpret_cast<C*>(smem_raw);
-  C* sl = sx + (1 << t);
-  double* red = reinterpret_cast<double*>(sl + (1 << t));
-  uint32_t* tbl = reinterpret_cast<uint32_t*>(red + 32 * kRedSlots);
-  // cotangent partial sums of this CTA's tiles (32 doubles per op of the
-  // pass), added to the instance's accumulators once per instance instead
-  // of one set of same-address global atomics per tile
-  double* stage = reinterpret_cast<double*>(tbl + (((1 << (t - c)) + 3) & ~3));
+  const int T = 1 << t;
   const int nops = pd.op_end - pd.op_begin;
-  // passes of several blocks: the state before block j is recomputed in a
-  // third tile from the state before the pass (blocks op_begin..j-1)
-  C* sw = reinterpret_cast<C*>(stage + 32 * nops);
-  for (int e = threadIdx.x; e < 32 * nops; e += blockDim.x) stage[e] = 0.0;
+  C* sl = reinterpret_cast<C*>(smem_raw);  // lambda
+  C* sw = sl + T;                          // state before the current block
+  C* slots = sw + T;                       // snapshots, nslot tiles
+  double* red = reinterpret_cast<double*>(slots + static_cast<size_t>(nslot) * T);
+  double* stage = red + 32 * kRedSlots;    // 32 doubles per op of the pass
+  uint32_t* tbl = reinterpret_cast<uint32_t*>(stage + 32 * nops);
+  int* snap_slot = reinterpret_cast<int*>(tbl + (((1 << (t - c)) + 3) & ~3));  // per op: slot of its input, -1
+  int* snap_pos = snap_slot + nops;                                             // per slot: op index
   fill_table(tbl, pd);
-  auto stage_slot = [&](const TileOp& op) -> bool {
-    // register-reduced forms only; wide blocks keep direct atomics
-    return (op.kind == BK_DENSE && op.kt <= 2) || (op.kind == BK_DIAG && op.kt <= 2);
-  };
+  for (int e = threadIdx.x; e < 32 * nops; e += blockDim.x) stage[e] = 0.0;
+  if (threadIdx.x == 0) {
+    // slot 0: the pass input (input of op 0); further slots: inputs of
+    // non-unitary ops, evenly spread when there are more than nslot - 1
+    int nc = 0;
+    for (int k = 1; k < nops; ++k) nc += ops[pd.op_begin + k].inv ? 0 : 1;
+    for (int k = 0; k < nops; ++k) snap_slot[k] = -1;
+    snap_slot[0] = 0;
+    snap_pos[0] = 0;
+    int used = 1, seen = 0;
+    for (int k = 1; k < nops; ++k) {
+      if (ops[pd.op_begin + k].inv) continue;
+      // candidate number `seen` of nc is taken when there is room for all of
+      // them, else when it is the next of nslot - 1 evenly spaced picks
+      if (used < nslot &&
+          (nc <= nslot - 1 || seen == static_cast<int>(static_cast<int64_t>(used - 1) * nc / (nslot - 1)))) {
+        snap_slot[k] = used;
+        snap_pos[used] = k;
+        ++used;
+      }
+      ++seen;
+    }
+    for (int j = used; j < nslot; ++j) snap_pos[j] = nops;  // unused
+  }
+  auto stage_slot = [&](const TileOp& op) -> bool { return op.kind == BK_DENSE && op.kt <= 2; };
+  auto diag_stage = [&](const TileOp& op) -> bool { return op.kind == BK_DIAG && op.kt <= 2; };
   auto flush = [&](int64_t inst) {
     __syncthreads();
     double* g = reinterpret_cast<double*>(gacc + inst * grad_stride);
     for (int k = 0; k < nops; ++k) {
       const TileOp& op = ops[pd.op_begin + k];
-      if (op.grad_off < 0 || !stage_slot(op)) continue;
+      if (op.grad_off < 0 || !(stage_slot(op) || diag_stage(op))) continue;
       const int nv = op.kind == BK_DENSE ? 2 * (1 << op.kt) * (1 << op.kt) : 2 * (1 << op.kt);
       for (int e = threadIdx.x; e < nv; e += blockDim.x) {
         atomicAdd(g + 2 * op.grad_off + e, stage[32 * k + e]);
@@ -1111,11 +1225,17 @@ __global__ void __launch_bounds__(512, 1) k_tile_bwd(const typename CplxT<R>::T*
     }
     __syncthreads();
   };
+  auto copy_tile = [&](C* dst, const C* src) {
+    constexpr int V = 16 / sizeof(C);
+    for (int v = threadIdx.x; v < T / V; v += blockDim.x)
+      reinterpret_cast<float4*>(dst)[v] = reinterpret_cast<const float4*>(src)[v];
+  };
   int64_t last_inst = -1;
   const int64_t tiles_per = 1LL << (nb - t);
   const int64_t ntiles = tiles_per * batch;
   const uint64_t full = (nb >= 64) ? ~0ULL : ((1ULL << nb) - 1);
   const uint64_t outer_mask = full & ~pd.tile_mask;
+  __syncthreads();
   for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const int64_t inst = tile >> (nb - t);
     const uint64_t ti = static_cast<uint64_t>(tile) & static_cast<uint64_t>(tiles_per - 1);
@@ -1127,36 +1247,59 @@ __global__ void __launch_bounds__(512, 1) k_tile_bwd(const typename CplxT<R>::T*
       last_inst = inst;
     }
     __syncthreads();
-    tile_load(sx, x + o, tbl, t, c);
+    tile_load(slots, x + o, tbl, t, c);
     tile_load(sl, lam + o, tbl, t, c);
     __syncthreads();
-    for (int oi = pd.op_end - 1; oi >= pd.op_begin; --oi) {
-      C* xs = sx;
-      if (oi > pd.op_begin) {
-        for (int e = threadIdx.x; e < (1 << t); e += blockDim.x) sw[e] = sx[e];
-        __syncthreads();
-        for (int k = pd.op_begin; k < oi; ++k) {
-          tile_apply<C>(sw, t, ops[k], bm, perms, false);
+    // forward walk: sw <- input of the last op, snapshots on the way
+    if (nops > 1) {
+      copy_tile(sw, slots);
+      __syncthreads();
+      for (int k = 0; k + 1 < nops; ++k) {
+        if (k > 0 && snap_slot[k] > 0) {
+          copy_tile(slots + static_cast<size_t>(snap_slot[k]) * T, sw);
           __syncthreads();
         }
-        xs = sw;
+        tile_apply<C>(sw, t, ops[pd.op_begin + k], bm, perms, false);
+        __syncthreads();
       }
-      TileOp op = ops[oi];
+    }
+    // reverse walk
+    for (int k = nops - 1; k >= 0; --k) {
+      const C* xs = nops > 1 ? sw : slots;
+      TileOp op = ops[pd.op_begin + k];
       if (!ga) op.grad_off = -1;
+      double* st = stage + 32 * k;
       switch (op.kind) {
         case BK_DENSE:
           switch (op.kt) {
-            case 1: bwd_dense<C, 1>(xs, sl, t, op, bm + op.mat_off, ga, red, stage + 32 * (oi - pd.op_begin)); break;
-            case 2: bwd_dense<C, 2>(xs, sl, t, op, bm + op.mat_off, ga, red, stage + 32 * (oi - pd.op_begin)); break;
+            case 1: bwd_dense_rs<C, 1>(xs, sl, t, op, bm + op.mat_off, ga ? st : nullptr); break;
+            case 2: bwd_dense_rs<C, 2>(xs, sl, t, op, bm + op.mat_off, ga ? st : nullptr); break;
             default: bwd_dense_wide<C>(xs, sl, t, op, bm + op.mat_off, ga); break;
           }
           break;
         case BK_DIAG:
-          bwd_diag<C>(xs, sl, t, op, bm + op.mat_off, ga, red, op.kt <= 2 ? stage + 32 * (oi - pd.op_begin) : nullptr);
+          bwd_diag<C>(xs, sl, t, op, bm + op.mat_off, ga, red, op.kt <= 2 ? st : nullptr);
           break;
         default: tile_apply<C>(sl, t, op, bm, perms, true); break;
       }
       __syncthreads();
+      if (k == 0 || nops == 1) continue;
+      // sw <- input of op k - 1
+      const TileOp& prev = ops[pd.op_begin + k - 1];
+      if (prev.inv) {
+        tile_apply<C>(sw, t, prev, bm, perms, true);
+        __syncthreads();
+        continue;
+      }
+      int j = 0;  // the nearest snapshot at or before op k - 1
+      for (int q = 1; q < nslot; ++q)
+        if (snap_pos[q] <= k - 1) j = q;
+      copy_tile(sw, slots + static_cast<size_t>(j) * T);
+      __syncthreads();
+      for (int q = snap_pos[j]; q < k - 1; ++q) {
+        tile_apply<C>(sw, t, ops[pd.op_begin + q], bm, perms, false);
+        __syncthreads();
+      }
     }
     tile_store(sl, lam + o, tbl, t, c);
   }
@@ -2372,13 +2515,32 @@ int backward_impl(const jq_plan* plan, int batch, const double* angles, const vo
       const PassDesc& pd = sch.passes[p];
       if (pd.op_end == pd.op_begin) continue;
       const int nops = pd.op_end - pd.op_begin;
-      const size_t smem = tile_smem<R>(pd, 2) + 16 + 32 * sizeof(double) * static_cast<size_t>(nops) +
-                          (nops > 1 ? (static_cast<size_t>(1) << pd.t) * sizeof(C) : 0);
+      // lambda + work tile + snapshot slots, reduction scratch, cotangent
+      // staging, bit-deposit table, snapshot tables
+      const size_t tile = (static_cast<size_t>(1) << pd.t) * sizeof(C);
+      const size_t fixed = 2 * tile + 32 * kRedSlots * sizeof(double) + 32 * sizeof(double) * nops +
+                           ((static_cast<size_t>(1) << (pd.t - pd.c)) + 3) / 4 * 16 + 8 * (nops + kMaxBwdSlots);
+      const size_t budget = 227 * 1024;
+      if (fixed + tile > budget) {
+        set_error("jq_backward: tile of " + std::to_string(pd.t) + " bits does not fit the reverse pass");
+        return JQ_EUNSUPPORTED;
+      }
+      const int nslot = static_cast<int>(std::min<size_t>({static_cast<size_t>(nops), static_cast<size_t>(kMaxBwdSlots),
+                                                           (budget - fixed) / tile}));
+      const size_t smem = fixed + static_cast<size_t>(nslot) * tile;
       const int64_t ntiles = (1LL << (plan->n_bits - pd.t)) * batch;
+      if (jm && jm->has_backward && jm->bfn[p]) {
+        // the pass specialised for this plan (NVRTC)
+        if ((rc = jit_launch_bwd(*jm, sch, static_cast<int>(p), plan->n_bits, sm_count(), seg(p - p0), lam, batch,
+                                 bmat, plan->bmat_stride, want_grad ? reinterpret_cast<double*>(gacc) : nullptr,
+                                 plan->grad_stride, static_cast<int>(sizeof(C)), st)))
+          return rc;
+        continue;
+      }
       const int ctas = ctas_for(k_tile_bwd<R>, plan->threads, smem, ntiles);
       k_tile_bwd<R><<<ctas, plan->threads, smem, st>>>(seg(p - p0), lam, plan->n_bits, batch, pd, sops, bmat,
                                                         plan->bmat_stride, T->perm_pool, want_grad ? gacc : nullptr,
-                                                        plan->grad_stride);
+                                                        plan->grad_stride, nslot);
     }
     JQ_CUDA(cudaGetLastError());
   }

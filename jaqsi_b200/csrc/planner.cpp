@@ -45,6 +45,7 @@ struct HostBlock {
   std::vector<int> wires;
   Structure st;
   std::vector<int> prims;
+  bool unitary = true;  // every prim is a unitary gate: the block is undone exactly by its dagger
 };
 
 std::vector<cd> read_matrix(const double* p, int dim) {
@@ -217,6 +218,7 @@ Schedule schedule(const std::vector<HostBlock>& blocks, const std::vector<DevBlo
       op.mat_off = db.mat_off;
       op.perm_off = db.perm_off;
       op.grad_off = db.grad_off;
+      op.inv = blocks[b].unitary ? 1 : 0;
       s.ops.push_back(op);
     }
     pd.op_end = static_cast<int32_t>(s.ops.size());
@@ -596,15 +598,20 @@ int build_plan(const jq_op* ops, int n_ops, const jq_obs* obs, int n_obs, int n_
       if (merge)
         for (int w : p.wires)
           if (last[w] != bi) { merge = false; break; }
+      // per-call matrices are not trusted to be exactly unitary (the caller's data)
+      const bool pu = p.op >= 0 && ops[p.op].unitary && ops[p.op].kind != JQ_K_CHANNEL &&
+                      ops[p.op].kind != JQ_K_MATRIX;
       if (merge) {
         blocks[bi].st = fused_structure(blocks[bi].st, p.st);
         blocks[bi].prims.push_back(pi);
+        blocks[bi].unitary = blocks[bi].unitary && pu;
         continue;
       }
       HostBlock b;
       b.wires = p.wires;
       b.st = p.st;
       b.prims.push_back(pi);
+      b.unitary = pu;
       blocks.push_back(std::move(b));
       for (int w : p.wires) last[w] = static_cast<int>(blocks.size()) - 1;
     }
