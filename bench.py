@@ -968,7 +968,7 @@ def main():
                     help="run only the batched-adjoint leg on one GPU and print its JSON (profiling runs)")
     ap.add_argument("--shift-sample", type=int, default=24,
                     help="instances whose parameter-shift baseline is timed and scaled")
-    ap.add_argument("--dm-sets", type=int, default=8, help="parameter sets of the noisy density-matrix leg")
+    ap.add_argument("--dm-sets", type=int, default=64, help="parameter sets of the noisy density-matrix leg")
     args = ap.parse_args()
     if args.impl == "reference":
         return reference_arm(args)
