@@ -749,15 +749,21 @@ def adjoint_20q_leg(dev, steps, cpu, hbm_peak, l2_gbs):
     return out
 
 
-def noisy_dm_leg(dev, sets, steps, cpu, hbm_peak):
+def noisy_dm_leg(dev, sets, steps, cpu, hbm_peak, world=1, max_over_ranks=None):
     """12-qubit density matrix, 20 layers of RX/RY/RZ on every wire + CX
     ring, DepolarizingChannel(0.01) then AmplitudeDamping(0.005) on every
     wire each gate touches, sum_i <Z_i>: forward + checkpointed reverse
     gradient of `sets` seeded parameter sets per step through
-    Script.execute(in_axes=(0,)) and backward, complex128 and complex64."""
+    Script.execute(in_axes=(0,)) and backward, complex128 and complex64.
+    With N ranks the parameter sets split over the ranks (jaqsi_b200.shard:
+    rows per rank, all-gather of the results, all-reduce of the gradients);
+    the time is the max over ranks."""
+    import contextlib
+
     import torch
 
     import jaqsi_b200 as jq
+    from jaqsi_b200 import shard
     from jaqsi_b200 import simulation as sim
     from jaqsi_b200 import workloads as W
 
@@ -769,6 +775,7 @@ def noisy_dm_leg(dev, sets, steps, cpu, hbm_peak):
     fd = _central_differences(script, obs, ang[0], idx)
     out = {"workload": f"12-qubit density matrix (4096 x 4096), 20 layers RX/RY/RZ + CX ring, depolarizing 0.01 + "
                        f"amplitude damping 0.005 after every gate, sum <Z_i>, {sets} parameter sets per step",
+           "sharding": f"parameter sets split over {world} ranks, time = max over ranks" if world > 1 else "1 GPU",
            "timed": "forward + checkpointed reverse: public API (Script.execute(in_axes) + backward) and "
                     "device-only (jq_forward + jq_backward, one parameter set)"}
     evs = {}
@@ -778,11 +785,14 @@ def noisy_dm_leg(dev, sets, steps, cpu, hbm_peak):
 
         def step():
             p.grad = None
-            ev = script.execute("expval", obs, args=(p,), in_axes=(0,), dtype=dt)
-            ev.sum().backward()
+            with shard.batch_sharding() if world > 1 else contextlib.nullcontext():
+                ev = script.execute("expval", obs, args=(p,), in_axes=(0,), dtype=dt)
+                ev.sum().backward()
             holder["ev"] = ev
 
         ms = _event_ms(step, steps, warmup=1)
+        if max_over_ranks is not None:
+            ms = max_over_ranks(ms)
         evs[name] = holder["ev"][0].detach().cpu().numpy().copy()
         g0 = p.grad[0].detach().cpu().numpy().reshape(-1)
         plan, lw = _plan_for(script, (torch.tensor(ang[0]),), obs, dt, n)
@@ -912,7 +922,7 @@ def ours_arm(args):
         t0 = time.perf_counter()
         result["adjoint_20q"] = adjoint_20q_leg(dev, max(3, args.steps // 2), cpu, peak, l2)
         t1 = time.perf_counter()
-        result["noisy_dm_12q"] = noisy_dm_leg(dev, args.dm_sets, 1, cpu, peak)
+        result["noisy_dm_12q"] = noisy_dm_leg(dev, args.dm_sets, 1, cpu, peak, world, max_over_ranks)
         t2 = time.perf_counter()
         result["small_10q"] = small_10q_leg(dev, max(5, args.steps), cpu)
         print(f"[bench] 20-qubit adjoint leg {t1 - t0:.1f} s, noisy density leg {t2 - t1:.1f} s",

@@ -30,7 +30,7 @@ import torch
 from torch.overrides import TorchFunctionMode
 
 from jaqsi_b200 import _lib as L
-from jaqsi_b200 import simulation
+from jaqsi_b200 import shard, simulation
 from jaqsi_b200.operations import Operation, rdtype
 from jaqsi_b200.tape import recording
 
@@ -326,6 +326,14 @@ class Script:
                 "Provide one in_axes entry per positional argument."
             )
         batch = self._batch_size(args, in_axes)
+        spec = shard.active()
+        if spec is not None and shots is None and batch >= spec[2]:
+            # this rank's rows of the batch, all-gathered (jaqsi_b200.shard)
+            def local(largs, lbatch, linit):
+                return self._execute_batched(type, obs, largs, kwargs, in_axes, None, key, linit, fingerprint,
+                                             dtype)
+
+            return shard.sharded_batch_call(local, args, in_axes, batch, *spec, initial_state=initial_state)
         dt = simulation._resolve_dtype(dtype)
         dev = simulation._device()
         tkey = self._trace_key(type, args, kwargs, in_axes, fingerprint, dtype, initial_state, shots)
