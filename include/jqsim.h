@@ -50,6 +50,9 @@ extern "C" {
 #define JQ_EABORT (-5)       /* the host abort flag was raised                */
 #define JQ_EUNSUPPORTED (-6) /* valid input outside what this build supports */
 
+/* init_batched flag of a density plan: `init` holds density matrices. */
+#define JQ_INIT_DENSITY 2
+
 /* ---- limits -------------------------------------------------------------- */
 #define JQ_MAX_OP_WIRES 6 /* widest gate / observable (matrix 64 x 64)      */
 #define JQ_MAX_QUBITS 30  /* statevector; density matrices up to 15 qubits  */
@@ -194,7 +197,11 @@ JQ_API size_t jq_workspace_bytes(const jq_plan* plan, int batch, int out_type,
  *   angles   float64 [batch, n_angles] (device) or NULL if n_angles == 0
  *   mats     complex128 [batch, n_mats] (device) or NULL if n_mats == 0
  *   init     NULL (|0..0>) or complex (run dtype) statevector(s):
- *            [2^n] broadcast when init_batched == 0, else [batch, 2^n]
+ *            [2^n] broadcast when init_batched bit 0 is clear, else
+ *            [batch, 2^n]; for a density plan with init_batched bit 1
+ *            (JQ_INIT_DENSITY) set, density matrices [2^n, 2^n] (or
+ *            [batch, 2^n, 2^n]) instead, copied as the initial state (the
+ *            reverse pass then returns the cotangent of that matrix)
  *   state    complex (run dtype) [batch, state_elems]: receives psi or rho
  *   out      EXPVAL: float64 [batch, n_obs]; PROBS: real run dtype
  *            [batch, 2^n]; DENSITY (pure): complex [batch, 4^n];

@@ -2281,8 +2281,10 @@ int forward_impl(const jq_plan* plan, int batch, const double* angles, const voi
   C* S = static_cast<C*>(state);
   const bool dm = plan->mode == JQ_DENSITY;
   const int64_t dim = 1LL << plan->n_qubits;
+  const bool init_rho = dm && init && (init_batched & JQ_INIT_DENSITY);  // init is a density matrix
   k_init<R><<<grid_for(plan->state_elems * batch, 256), 256, 0, st>>>(
-      S, plan->state_elems, batch, static_cast<const C*>(init), dim, init_batched, dm && init ? 1 : 0);
+      S, plan->state_elems, batch, static_cast<const C*>(init), init_rho ? plan->state_elems : dim,
+      init_batched & 1, dm && init && !init_rho ? 1 : 0);
   JQ_CUDA(cudaGetLastError());
   if ((rc = run_passes<R>(plan, plan->fwd, T->fwd_ops, T->fwd_steps, T->fwd_rops, T, S, batch, bmat, 0, plan->fwd.passes.size(), st,
                           static_cast<const JitModule*>(T->jit)))) return rc;
@@ -2481,8 +2483,10 @@ int backward_impl(const jq_plan* plan, int batch, const double* angles, const vo
   if ((rc = prep<R>(plan, T, batch, angles, mats, bmat, scratch, st))) return rc;
   const bool dm = plan->mode == JQ_DENSITY;
   const int64_t dim = 1LL << plan->n_qubits;
-  k_init<R><<<grid_for(elems * batch, 256), 256, 0, st>>>(work, elems, batch, static_cast<const C*>(init), dim,
-                                                          init_batched, dm && init ? 1 : 0);
+  const bool init_rho = dm && init && (init_batched & JQ_INIT_DENSITY);  // init is a density matrix
+  k_init<R><<<grid_for(elems * batch, 256), 256, 0, st>>>(work, elems, batch, static_cast<const C*>(init),
+                                                          init_rho ? elems : dim, init_batched & 1,
+                                                          dm && init && !init_rho ? 1 : 0);
   JQ_CUDA(cudaGetLastError());
   // The reverse walks the fused forward schedule: checkpoints every S passes,
   // recompute of a segment with the (specialised) forward passes, and one
@@ -2545,12 +2549,15 @@ int backward_impl(const jq_plan* plan, int batch, const double* angles, const vo
     JQ_CUDA(cudaGetLastError());
   }
   if (grad_init) {
-    if (dm) {
+    if (init_rho) {
+      // the cotangent of an initial density matrix is lambda itself
+      JQ_CUDA(cudaMemcpyAsync(grad_init, lam, sizeof(C) * elems * batch, cudaMemcpyDeviceToDevice, st));
+    } else if (dm) {
       if (!init) {
         set_error("grad_init requested without an initial state");
         return JQ_EINVAL;
       }
-      k_grad_init_dm<R><<<grid_for(dim * batch, 256), 256, 0, st>>>(lam, static_cast<const C*>(init), init_batched,
+      k_grad_init_dm<R><<<grid_for(dim * batch, 256), 256, 0, st>>>(lam, static_cast<const C*>(init), init_batched & 1,
                                                                      static_cast<C*>(grad_init), dim, batch);
       JQ_CUDA(cudaGetLastError());
     } else {

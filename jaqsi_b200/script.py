@@ -46,6 +46,14 @@ _VALUE_READS = frozenset(
 _NO_TRACE = object()
 
 
+def _transformed(t: torch.Tensor) -> bool:
+    """Whether t is wrapped by a torch.func transform (vmap, grad, jvp, ...)."""
+    try:
+        return bool(torch._C._functorch.is_functorch_wrapped_tensor(t))
+    except AttributeError:  # pragma: no cover - older torch
+        return False
+
+
 def _tensors_in(x):
     if isinstance(x, torch.Tensor):
         yield x
@@ -272,6 +280,8 @@ class Script:
         sig = []
         for i, a in enumerate(args):
             if isinstance(a, torch.Tensor):
+                if _transformed(a):
+                    return None  # under a torch.func transform: record every call
                 sig.append(("t", tuple(a.shape), a.dtype, a.device, a.requires_grad))
             elif a is None or isinstance(a, (bool, int, float, complex, str)):
                 if in_axes is not None and in_axes[i] is not None:

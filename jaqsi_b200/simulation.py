@@ -426,6 +426,13 @@ def get_plan(lw: Lowered, obs_specs, obs_key, n_qubits: int, mode: int, dtype: t
     return plan
 
 
+def _functorch_wrapped(t: torch.Tensor) -> bool:
+    try:
+        return bool(torch._C._functorch.is_functorch_wrapped_tensor(t))
+    except AttributeError:  # pragma: no cover - older torch
+        return False
+
+
 def _view_gather(values: list, device: torch.device) -> Optional[torch.Tensor]:
     """One index op when every tensor angle is a one-element view of the same
     contiguous base tensor (the ``params[l, w, i]`` pattern); None otherwise.
@@ -441,8 +448,11 @@ def _view_gather(values: list, device: torch.device) -> Optional[torch.Tensor]:
         if isinstance(v, tensor):
             b = v._base
             if b is not base:
-                # first tensor angle: the base is checked once
+                # first tensor angle: the base is checked once (views made
+                # under a torch.func transform carry no usable offsets)
                 if base is not None or b is None or not b.is_floating_point() or not b.is_contiguous():
+                    return None
+                if _functorch_wrapped(v):
                     return None
                 base, dtype = b, b.dtype
             if v.dtype is not dtype or v.numel() != 1:
@@ -508,91 +518,272 @@ def _stream() -> ctypes.c_void_p:
     return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
 
 
+# init_batched flag: the initial state of a density plan is a density matrix
+_INIT_DENSITY = 2
+
+
+def _returns_state(plan: Plan, out_type: int) -> bool:
+    return out_type == L.JQ_OUT_STATE or (out_type == L.JQ_OUT_DENSITY and plan.mode == L.JQ_DENSITY)
+
+
+def _forward_launch(plan: Plan, out_type: int, batch: int, init_batched: int, angles, mats, init):
+    """jq_forward into fresh (state, out) tensors."""
+    dev = _device()
+    dim = 1 << plan.n_qubits
+    shape = (batch, dim, dim) if plan.mode == L.JQ_DENSITY else (batch, dim)
+    state = torch.empty(shape, dtype=plan.cdtype, device=dev)
+    out = None
+    if out_type == L.JQ_OUT_EXPVAL:
+        out = torch.empty((batch, plan.n_obs), dtype=torch.float64, device=dev)
+    elif out_type == L.JQ_OUT_PROBS:
+        out = torch.empty((batch, dim), dtype=plan.rdtype, device=dev)
+    elif out_type == L.JQ_OUT_DENSITY and plan.mode == L.JQ_STATEVECTOR:
+        out = torch.empty((batch, dim, dim), dtype=plan.cdtype, device=dev)
+    wsb = plan.workspace_bytes(batch, 0)
+    ws = torch.empty(max(wsb, 1), dtype=torch.uint8, device=dev)
+    L.check(
+        plan._lib.jq_forward(
+            plan.handle, batch, _ptr(angles), _ptr(mats), _ptr(init), init_batched, out_type,
+            _ptr(state), _ptr(out), _ptr(ws), wsb, _stream(),
+        )
+    )
+    return state, out
+
+
 class _Execute(torch.autograd.Function):
-    """Forward = jq_forward; backward = jq_adjoint or jq_backward."""
+    """Forward = jq_forward; backward = jq_adjoint or jq_backward (through
+    _ExecuteGrad); forward-mode derivatives (torch.func.jvp / jacfwd) through
+    `jvp`.  The second output is the final state for the derivative rules
+    (empty when the result is the state itself); run_plan drops it."""
 
     @staticmethod
-    def forward(ctx, plan: Plan, out_type: int, batch: int, init_batched: int, angles, mats, init):
-        dev = _device()
-        lib = plan._lib
-        dim = 1 << plan.n_qubits
-        shape = (batch, dim, dim) if plan.mode == L.JQ_DENSITY else (batch, dim)
-        state = torch.empty(shape, dtype=plan.cdtype, device=dev)
-        out = None
-        if out_type == L.JQ_OUT_EXPVAL:
-            out = torch.empty((batch, plan.n_obs), dtype=torch.float64, device=dev)
-        elif out_type == L.JQ_OUT_PROBS:
-            out = torch.empty((batch, dim), dtype=plan.rdtype, device=dev)
-        elif out_type == L.JQ_OUT_DENSITY and plan.mode == L.JQ_STATEVECTOR:
-            out = torch.empty((batch, dim, dim), dtype=plan.cdtype, device=dev)
-        wsb = plan.workspace_bytes(batch, 0)
-        ws = torch.empty(max(wsb, 1), dtype=torch.uint8, device=dev)
+    def forward(plan: Plan, out_type: int, batch: int, init_batched: int, angles, mats, init):
+        state, out = _forward_launch(plan, out_type, batch, init_batched, angles, mats, init)
+        if _returns_state(plan, out_type):
+            return state, state.new_empty(0)
+        return out, state
+
+    @staticmethod
+    def setup_context(ctx, inputs, output):
+        plan, out_type, batch, init_batched, angles, mats, init = inputs
+        res, aux = output
+        state = res if aux.numel() == 0 else aux
+        ctx.mark_non_differentiable(aux)
+        ctx.plan, ctx.out_type, ctx.batch, ctx.init_batched = plan, out_type, batch, init_batched
+        ctx.save_for_backward(angles, mats, init, state)
+        ctx.save_for_forward(angles, mats, init, state)
+
+    @staticmethod
+    def backward(ctx, g, _g_aux):
+        angles, mats, init, state = ctx.saved_tensors
+        need = (angles is not None and ctx.needs_input_grad[4], mats is not None and ctx.needs_input_grad[5],
+                init is not None and ctx.needs_input_grad[6])
+        if not any(need):
+            return None, None, None, None, None, None, None
+        ga, gm, gi = _ExecuteGrad.apply(ctx.plan, ctx.out_type, ctx.batch, ctx.init_batched, need, angles, mats,
+                                        init, state, g)
+        return (None, None, None, None) + _shape_grads(ctx.init_batched, need, angles, mats, ga, gm, gi)
+
+    @staticmethod
+    def vmap(info, in_dims, plan, out_type, batch, init_batched, angles, mats, init):
+        """Batched inputs become extra plan instances: vmap index v, instance
+        b -> instance v * batch + b."""
+        B = info.batch_size
+        da, dm, di = in_dims[4], in_dims[5], in_dims[6]
+        fold = _vmap_folder(B, batch)
+        ang = None if angles is None else fold(angles, da, (angles.dim() - (da is not None)) == 1)
+        mt = None if mats is None else fold(mats, dm, (mats.dim() - (dm is not None)) == 1)
+        ini, ib = init, init_batched
+        if init is not None and (di is not None or init_batched & 1):
+            ini = fold(init, di, not init_batched & 1)
+            ib = init_batched | 1
+        res, aux = _Execute.apply(plan, out_type, B * batch, ib, ang, mt, ini)
+        res = res.reshape((B, batch) + tuple(res.shape[1:]))
+        if aux.numel():
+            aux = aux.reshape((B, batch) + tuple(aux.shape[1:]))
+            return (res, aux), (0, 0)
+        return (res, aux), (0, None)
+
+    @staticmethod
+    def jvp(ctx, _t_plan, _t_out, _t_batch, _t_initb, t_angles, t_mats, t_init):
+        """Tangent of the result: J v, with the rows of J from one batched
+        reverse call (one instance per real output component).  jaqsi routes
+        forward mode around its adjoint into plain autodiff
+        (jaqsi/simulation.py:492-518); here the adjoint supplies the rows."""
+        angles, mats, init, state = ctx.saved_tensors
+        plan, out_type, batch = ctx.plan, ctx.out_type, ctx.batch
+        return _jvp_by_rows(plan, out_type, batch, ctx.init_batched, angles, mats, init, state, t_angles, t_mats,
+                            t_init), None
+
+
+def _shape_grads(init_batched, need, angles, mats, ga, gm, gi):
+    ga = ga if need[0] else None
+    gm = gm if need[1] else None
+    gi = gi if need[2] else None
+    if gi is not None and not init_batched & 1:
+        gi = gi.sum(0)
+    if ga is not None and angles.dim() == 1:
+        ga = ga[0]
+    if gm is not None and mats.dim() == 1:
+        gm = gm[0]
+    return ga, gm, gi
+
+
+def _grad_launch(plan: Plan, out_type: int, batch: int, init_batched: int, need, angles, mats, init, state, g):
+    """Per-instance input gradients [batch, ...] for the output cotangent g."""
+    dev = state.device
+    lib = plan._lib
+    g = g.contiguous()
+    ct = g.to(torch.float64).contiguous() if out_type == L.JQ_OUT_EXPVAL else None
+    ct_state = None
+    if out_type != L.JQ_OUT_EXPVAL:
+        ct_state = g.to(plan.rdtype if out_type == L.JQ_OUT_PROBS else plan.cdtype).contiguous()
+    ga = torch.empty((batch, plan.n_angles), dtype=torch.float64, device=dev) if need[0] else None
+    gm = torch.empty((batch, plan.n_mats), dtype=torch.complex128, device=dev) if need[1] else None
+    gdim = plan.state_elems if init_batched & _INIT_DENSITY else 1 << plan.n_qubits
+    gi = torch.empty((batch, gdim), dtype=plan.cdtype, device=dev) if need[2] else None
+    use_adjoint = plan.mode == L.JQ_STATEVECTOR and plan.unitary
+    wsb = plan.workspace_bytes(batch, 1 if use_adjoint else 2)
+    ws = torch.empty(max(wsb, 1), dtype=torch.uint8, device=dev)
+    if use_adjoint:
         L.check(
-            lib.jq_forward(
-                plan.handle, batch, _ptr(angles), _ptr(mats), _ptr(init), init_batched, out_type,
-                _ptr(state), _ptr(out), _ptr(ws), wsb, _stream(),
+            lib.jq_adjoint(
+                plan.handle, batch, _ptr(angles), _ptr(mats), _ptr(state), out_type, _ptr(ct),
+                _ptr(ct_state), _ptr(ga), _ptr(gm), _ptr(gi), _ptr(ws), wsb, _stream(),
             )
         )
-        ctx.plan = plan
-        ctx.out_type = out_type
-        ctx.batch = batch
-        ctx.init_batched = init_batched
-        ctx.save_for_backward(angles, mats, init, state)
-        if out_type == L.JQ_OUT_STATE or (out_type == L.JQ_OUT_DENSITY and plan.mode == L.JQ_DENSITY):
-            return state
-        return out
+    else:
+        L.check(
+            lib.jq_backward(
+                plan.handle, batch, _ptr(angles), _ptr(mats), _ptr(init), init_batched, out_type,
+                _ptr(ct), _ptr(ct_state), _ptr(ga), _ptr(gm), _ptr(gi), _ptr(ws), wsb, _stream(),
+            )
+        )
+    empty = torch.empty(0, device=dev)
+    return (ga if ga is not None else empty, gm if gm is not None else empty, gi if gi is not None else empty)
+
+
+class _ExecuteGrad(torch.autograd.Function):
+    """The reverse call as its own Function so that torch.func transforms
+    can batch it (`vmap`: jacrev's stacked cotangents become extra plan
+    instances).  No second derivatives."""
 
     @staticmethod
-    def backward(ctx, g):
-        plan: Plan = ctx.plan
-        angles, mats, init, state = ctx.saved_tensors
-        need_ang = angles is not None and ctx.needs_input_grad[4]
-        need_mat = mats is not None and ctx.needs_input_grad[5]
-        need_init = init is not None and ctx.needs_input_grad[6]
-        if not (need_ang or need_mat or need_init):
-            return None, None, None, None, None, None, None
-        dev = state.device
-        batch = ctx.batch
-        lib = plan._lib
-        g = g.contiguous()
-        ct = g if ctx.out_type == L.JQ_OUT_EXPVAL else None
-        ct_state = None if ctx.out_type == L.JQ_OUT_EXPVAL else g
-        if ct is not None:
-            ct = ct.to(torch.float64)
-        if ct_state is not None:
-            ct_state = ct_state.to(plan.rdtype if ctx.out_type == L.JQ_OUT_PROBS else plan.cdtype).contiguous()
-        ga = torch.empty((batch, plan.n_angles), dtype=torch.float64, device=dev) if need_ang else None
-        gm = torch.empty((batch, plan.n_mats), dtype=torch.complex128, device=dev) if need_mat else None
-        gi = torch.empty((batch, 1 << plan.n_qubits), dtype=plan.cdtype, device=dev) if need_init else None
-        use_adjoint = plan.mode == L.JQ_STATEVECTOR and plan.unitary
-        wsb = plan.workspace_bytes(batch, 1 if use_adjoint else 2)
-        ws = torch.empty(max(wsb, 1), dtype=torch.uint8, device=dev)
-        if use_adjoint:
-            L.check(
-                lib.jq_adjoint(
-                    plan.handle, batch, _ptr(angles), _ptr(mats), _ptr(state), ctx.out_type, _ptr(ct),
-                    _ptr(ct_state), _ptr(ga), _ptr(gm), _ptr(gi), _ptr(ws), wsb, _stream(),
-                )
-            )
-        else:
-            L.check(
-                lib.jq_backward(
-                    plan.handle, batch, _ptr(angles), _ptr(mats), _ptr(init), ctx.init_batched, ctx.out_type,
-                    _ptr(ct), _ptr(ct_state), _ptr(ga), _ptr(gm), _ptr(gi), _ptr(ws), wsb, _stream(),
-                )
-            )
-        if gi is not None and not ctx.init_batched:
-            gi = gi.sum(0)
-        if ga is not None and angles.dim() == 1:
-            ga = ga[0]
-        if gm is not None and mats.dim() == 1:
-            gm = gm[0]
-        return None, None, None, None, ga, gm, gi
+    def forward(plan, out_type, batch, init_batched, need, angles, mats, init, state, g):
+        return _grad_launch(plan, out_type, batch, init_batched, need, angles, mats, init, state, g)
+
+    @staticmethod
+    def setup_context(ctx, inputs, output):
+        pass
+
+    @staticmethod
+    def backward(ctx, *grads):
+        raise RuntimeError("second derivatives through a simulated circuit are not supported")
+
+    @staticmethod
+    def vmap(info, in_dims, plan, out_type, batch, init_batched, need, angles, mats, init, state, g):
+        """Batched inputs (jacrev's stacked cotangents, or circuit inputs)
+        become extra plan instances: vmap index v, instance b -> v * batch + b."""
+        B = info.batch_size
+        da, dm, di, ds, dg = in_dims[5:10]
+        fold = _vmap_folder(B, batch)
+        ang = None if angles is None else fold(angles, da, (angles.dim() - (da is not None)) == 1)
+        mt = None if mats is None else fold(mats, dm, (mats.dim() - (dm is not None)) == 1)
+        ini, ib = init, init_batched
+        if init is not None and (di is not None or init_batched & 1):
+            ini = fold(init, di, not init_batched & 1)
+            ib = init_batched | 1
+        ga, gm, gi = _ExecuteGrad.apply(plan, out_type, B * batch, ib, need, ang, mt, ini,
+                                        fold(state, ds, False), fold(g, dg, False))
+
+        def split(t):
+            return t if t.numel() == 0 else t.reshape((B, batch) + tuple(t.shape[1:]))
+
+        ga, gm, gi = split(ga), split(gm), split(gi)
+        return (ga, gm, gi), (0 if ga.numel() else None, 0 if gm.numel() else None, 0 if gi.numel() else None)
+
+
+def _vmap_folder(B: int, batch: int):
+    """fold(t, d, shared): a tensor of a vmapped Function call (vmap dim d,
+    None if unbatched) as [B * batch, ...] rows, one per plan instance; a
+    per-index tensor that is `shared` by the batch's instances is repeated."""
+
+    def fold(t, d, shared):
+        if t is None:
+            return None
+        t = t.unsqueeze(0).expand((B,) + tuple(t.shape)) if d is None else t.movedim(d, 0)
+        if shared:
+            return t.unsqueeze(1).expand(B, batch, *t.shape[1:]).reshape(B * batch, *t.shape[1:]).contiguous()
+        return t.reshape(B * batch, *t.shape[2:]).contiguous()
+
+    return fold
+
+
+# Forward-mode derivatives need one reverse instance per real output
+# component; beyond this many amplitudes in flight they are refused.
+_JVP_MAX_ELEMS = 1 << 28
+
+
+def _jvp_by_rows(plan: Plan, out_type: int, batch: int, init_batched: int, angles, mats, init, state,
+                 t_angles, t_mats, t_init):
+    dim = 1 << plan.n_qubits
+    if out_type == L.JQ_OUT_EXPVAL:
+        shape, cplx = (plan.n_obs,), False
+    elif out_type == L.JQ_OUT_PROBS:
+        shape, cplx = (dim,), False
+    elif out_type == L.JQ_OUT_STATE:
+        shape, cplx = (dim,), True
+    else:
+        shape, cplx = (dim, dim), True
+    n_out = int(np.prod(shape))
+    rows = n_out * (2 if cplx else 1)
+    if rows * batch * plan.state_elems > _JVP_MAX_ELEMS:
+        raise NotImplementedError(
+            f"forward-mode derivatives of this {'state' if cplx else 'output'} need {rows * batch} reverse passes "
+            f"over {plan.state_elems}-element states; use reverse mode (backward / jacrev)")
+    dev = state.device
+    # cotangents: instance (b, r) has a one-hot cotangent on real component r
+    eye = torch.eye(n_out, dtype=torch.float64, device=dev)
+    ct = eye if not cplx else torch.cat([eye.to(plan.cdtype), 1j * eye.to(plan.cdtype)])
+    ct = ct.reshape((rows,) + shape)
+    g = ct.unsqueeze(0).expand((batch,) + tuple(ct.shape)).reshape((batch * rows,) + shape)
+
+    def rep(t):
+        return None if t is None else t.unsqueeze(1).expand((t.shape[0], rows) + tuple(t.shape[1:])).reshape(
+            (t.shape[0] * rows,) + tuple(t.shape[1:]))
+
+    ang2 = angles if angles is None or angles.dim() == 2 else angles.unsqueeze(0).expand(batch, -1)
+    mat2 = mats if mats is None or mats.dim() == 2 else mats.unsqueeze(0).expand(batch, -1)
+    ini2 = init if init is None or init_batched & 1 else init.unsqueeze(0).expand(batch, -1)
+    need = (angles is not None and t_angles is not None, mats is not None and t_mats is not None,
+            init is not None and t_init is not None)
+    ga, gm, gi = _ExecuteGrad.apply(plan, out_type, batch * rows, 1 | (init_batched & _INIT_DENSITY), need,
+                                    None if ang2 is None else rep(ang2).contiguous(),
+                                    None if mat2 is None else rep(mat2).contiguous(),
+                                    None if ini2 is None else rep(ini2).contiguous(), rep(state).contiguous(), g)
+    tan = torch.zeros((batch, rows), dtype=torch.float64, device=dev)
+    if need[0]:
+        ta = t_angles if t_angles.dim() == 2 else t_angles.unsqueeze(0).expand(batch, -1)
+        tan = tan + torch.einsum("bri,bi->br", ga.reshape(batch, rows, -1), ta.to(torch.float64))
+    if need[1]:
+        tm = t_mats if t_mats.dim() == 2 else t_mats.unsqueeze(0).expand(batch, -1)
+        tan = tan + torch.einsum("bri,bi->br", gm.reshape(batch, rows, -1).conj(), tm.to(torch.complex128)).real
+    if need[2]:
+        ti = t_init if init_batched & 1 else t_init.unsqueeze(0).expand(batch, -1)
+        tan = tan + torch.einsum("bri,bi->br", gi.reshape(batch, rows, -1).conj().to(torch.complex128),
+                                 ti.to(torch.complex128)).real
+    if cplx:
+        tan = torch.complex(tan[:, :n_out], tan[:, n_out:])
+    tan = tan.reshape((batch,) + shape)
+    if out_type == L.JQ_OUT_EXPVAL:
+        return tan
+    rd = plan.rdtype if not cplx else plan.cdtype
+    return tan.to(rd)
 
 
 def run_plan(plan: Plan, out_type: int, batch: int, angles, mats, init, init_batched: int) -> torch.Tensor:
     """Execute *plan* for *batch* instances through the autograd Function."""
-    return _Execute.apply(plan, out_type, batch, init_batched, angles, mats, init)
+    return _Execute.apply(plan, out_type, batch, init_batched, angles, mats, init)[0]
 
 
 def _prepare_init(initial_state, n_qubits: int, dtype: torch.dtype, device, batched_ok: bool):
@@ -728,10 +919,19 @@ def measure_density(rho: torch.Tensor, n_qubits: int, type: str, obs: List[Opera
     r = r.to(dt)
     if type == "density":
         return r
-    if type == "probs":
-        return torch.real(torch.diagonal(r, dim1=-2, dim2=-1))
-    mats = torch.stack([ob.lifted_matrix(n_qubits).to(device=r.device, dtype=dt) for ob in obs])
-    return torch.real(torch.einsum("oij,...ji->...o", mats, r.reshape(*r.shape[:-2], dim, dim)))
+    # an empty density plan run from rho: the GPU measurement kernels
+    # (Pauli words and dense observables on the density, its diagonal)
+    dev = _device()
+    batched = r.dim() == 3
+    batch = r.shape[0] if batched else 1
+    if r.shape[-2:] != (dim, dim):
+        raise ValueError(f"rho has shape {tuple(r.shape)}, expected (..., {dim}, {dim})")
+    rr = r.reshape(batch, dim * dim).to(dev).contiguous()
+    lw = lower_tape([], n_qubits)
+    specs, okey = _lower_obs(obs if type == "expval" else [], n_qubits)
+    plan = get_plan(lw, specs, okey, n_qubits, L.JQ_DENSITY, dt)
+    res = _finish(run_plan(plan, _OUT[type], batch, None, None, rr, 1 | _INIT_DENSITY), type, dt)
+    return res if batched else res[0]
 
 
 # ---------------------------------------------------------------------------
