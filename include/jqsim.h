@@ -333,6 +333,27 @@ JQ_API int jq_batch_run(jq_batch* batch, const double* angles, const double* ct,
 JQ_API int jq_batch_autotune(jq_batch* batch, const double* angles, double* expval, double* grad,
                              void* workspace, size_t workspace_bytes, void* stream, jq_batch_config* chosen);
 
+/* ------------------------------------------------------------------------
+ * Pulse-gate unitaries: ordered products of matrix exponentials, the form
+ * of every step of jaqsi's commutator-free Magnus integrators
+ * (jaqsi/evolution.py:195-264) that resolve_pending solves in batches for
+ * the pulse gates of a tape (jaqsi/evolution.py:730-773, called from
+ * jaqsi/simulation.py:713).  For gate g:
+ *   U[g] = expm(Om[g, M-1]) ... expm(Om[g, 0]),  Om[g, m] = sum_i w[g, m, i] A[g, i]
+ *   A      complex128 [n_gates][n_terms][dim][dim] (A_i = -i H_i), gate g at
+ *          A + 2 * g * a_stride doubles (a_stride complex elements; 0: shared)
+ *   w      complex128 [n_gates][n_sub][n_terms]
+ *   U      complex128 [n_gates][dim][dim] (written)
+ * dim is 2, 4 or 8; n_sub at most 2048 (dim <= 4) or 512 (dim 8).  Device
+ * pointers; no workspace.
+ * jq_magnus_product_grad: gw[g, m, i] = dL/dw[g, m, i] (complex128, written)
+ * from gU = dL/dU (complex128 [n_gates][dim][dim]), PyTorch's convention
+ * for complex gradients (d/dRe + i d/dIm). */
+JQ_API int jq_magnus_product(int n_gates, int dim, int n_terms, int n_sub, const double* A, int64_t a_stride,
+                             const double* w, double* U, void* stream);
+JQ_API int jq_magnus_product_grad(int n_gates, int dim, int n_terms, int n_sub, const double* A, int64_t a_stride,
+                                  const double* w, const double* gU, double* gw, void* stream);
+
 /* Message of the last failed call on this thread ("" if none). */
 JQ_API const char* jq_last_error(void);
 

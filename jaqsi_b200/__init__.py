@@ -20,6 +20,7 @@ from jaqsi_b200.script import Script, make_hashable
 from jaqsi_b200.tape import copy_to_tape, recording, shift_and_append
 from jaqsi_b200 import simulation
 from jaqsi_b200.batch import BatchedGradients
+from jaqsi_b200.evolution import Evolution, ParametrizedHamiltonian, PendingEvolution, resolve_pending
 
 __version__ = "0.1.0"
 
@@ -31,4 +32,5 @@ __all__ = [
     "ControlledPauliRot", "DiagonalQubitUnitary", "RandomUnitary", "Barrier",
     "KrausChannel", "BitFlip", "PhaseFlip", "DepolarizingChannel", "AmplitudeDamping", "PhaseDamping",
     "ThermalRelaxationError", "QubitChannel",
+    "Evolution", "ParametrizedHamiltonian", "PendingEvolution", "resolve_pending",
 ]

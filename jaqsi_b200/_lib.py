@@ -53,6 +53,8 @@ EXPORTED = (
     "jq_backward",
     "jq_sample_workspace_bytes",
     "jq_sample_shots",
+    "jq_magnus_product",
+    "jq_magnus_product_grad",
     "jq_batch_build",
     "jq_batch_free",
     "jq_batch_info",
@@ -187,6 +189,10 @@ def _declare(lib: ctypes.CDLL) -> None:
     lib.jq_sample_shots.argtypes = [vp, i32, ctypes.c_int64, ctypes.c_int64, ctypes.c_uint64, vp, vp,
                                     ctypes.c_size_t, vp]
     lib.jq_sample_shots.restype = i32
+    lib.jq_magnus_product.argtypes = [i32, i32, i32, i32, vp, ctypes.c_int64, vp, vp, vp]
+    lib.jq_magnus_product.restype = i32
+    lib.jq_magnus_product_grad.argtypes = [i32, i32, i32, i32, vp, ctypes.c_int64, vp, vp, vp, vp]
+    lib.jq_magnus_product_grad.restype = i32
     lib.jq_batch_build.argtypes = [ctypes.POINTER(vp), i32, ctypes.POINTER(ctypes.c_int32), i32,
                                    ctypes.POINTER(JqBatchConfig), ctypes.POINTER(vp)]
     lib.jq_batch_build.restype = i32

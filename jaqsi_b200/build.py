@@ -17,7 +17,7 @@ CSRC = os.path.join(HERE, "csrc")
 INCLUDE = os.path.join(HERE, "..", "include")
 OBJDIR = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libjqsim.so")
-SOURCES = ["planner.cpp", "jit.cpp", "jqsim.cu"]
+SOURCES = ["planner.cpp", "jit.cpp", "jqsim.cu", "pulse.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
          "--expt-relaxed-constexpr"]

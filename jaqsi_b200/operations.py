@@ -331,3 +331,20 @@ class Hermitian(Operation):
         if not isinstance(matrix, torch.Tensor):
             matrix = np.asarray(matrix, dtype=np.complex128)
         super().__init__(wires=wires, matrix=matrix, record=record)
+
+    def __rmul__(self, coeff_fn):
+        """``coeff_fn * Hermitian`` -> a one-term ParametrizedHamiltonian
+        (jaqsi/operations.py:683-702)."""
+        if isinstance(coeff_fn, Operation):
+            return Operation.__mul__(self, coeff_fn)
+        if not callable(coeff_fn):
+            raise TypeError(f"Left operand of `* Hermitian` must be callable, got {type(coeff_fn)}")
+        from jaqsi_b200.evolution import ParametrizedHamiltonian
+
+        return ParametrizedHamiltonian(terms=[(coeff_fn, self._matrix, self.wires)])
+
+    def evolve(self, name: Optional[str] = None, **odeint_kwargs):
+        """Gate factory ``(t, wires=0) -> exp(-i t H)`` (jaqsi/operations.py:704-720)."""
+        from jaqsi_b200.evolution import Evolution
+
+        return Evolution.evolve(self, name=name, **odeint_kwargs)

@@ -246,7 +246,11 @@ def _bad_wire(op, wires, n_qubits):
 
 
 def lower_tape(tape: Sequence[Operation], n_qubits: int) -> Lowered:
-    """Lower recorded ops to plan statics and per-call values."""
+    """Lower recorded ops to plan statics and per-call values.  Pending pulse
+    gates are solved first, in batches (jaqsi/simulation.py:713)."""
+    from jaqsi_b200.evolution import resolve_pending
+
+    resolve_pending(tape)
     lw = Lowered()
     keys = []
     statics = lw.statics

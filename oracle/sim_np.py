@@ -611,3 +611,51 @@ def jaqsi_plan(records, n: int, compose=None):
             run.append(b)
     flush()
     return plan
+
+
+# ---------------------------------------------------------------------------
+# pulse gates (jaqsi/evolution.py:195-264 Magnus schemes, :354-405 closed form)
+# ---------------------------------------------------------------------------
+def magnus_unitary(H_mats, fns, params, t0: float, t1: float, steps: int, order: int) -> np.ndarray:
+    """The reference's fixed-step commutator-free Magnus integrators: the
+    midpoint rule (order 2) or CFM4:2 with U <- exp(Om_b) exp(Om_a) U
+    (order 4); coefficient functions take (params, t) with float t."""
+    from scipy.linalg import expm
+
+    A = [-1j * np.asarray(H, dtype=np.complex128) for H in H_mats]
+    d = A[0].shape[0]
+    h = (t1 - t0) / steps
+
+    def Hat(t):
+        return sum(complex(f(p, t)) * a for f, p, a in zip(fns, params, A))
+
+    U = np.eye(d, dtype=np.complex128)
+    s3 = np.sqrt(3.0)
+    c1, c2, a1, a2 = 0.5 - s3 / 6, 0.5 + s3 / 6, 0.25 + s3 / 6, 0.25 - s3 / 6
+    for n in range(steps):
+        tn = t0 + n * h
+        if order == 2:
+            U = expm(h * Hat(tn + 0.5 * h)) @ U
+        else:
+            H1, H2 = Hat(tn + c1 * h), Hat(tn + c2 * h)
+            U = expm(h * (a2 * H1 + a1 * H2)) @ expm(h * (a1 * H1 + a2 * H2)) @ U
+    return U
+
+
+def evolution_reference(H_mats, fns, params, t0: float, t1: float, rtol: float = 1e-12) -> np.ndarray:
+    """dU/dt = -i sum_i f_i(p_i, t) H_i U, U(t0) = I, by an adaptive
+    Dormand-Prince (order 8) solve at tight tolerances: an independent check
+    of the Magnus schemes and the closed form."""
+    from scipy.integrate import solve_ivp
+
+    Hs = [np.asarray(H, dtype=np.complex128) for H in H_mats]
+    d = Hs[0].shape[0]
+
+    def rhs(t, y):
+        U = y.reshape(d, d)
+        Ht = sum(complex(f(p, t)) * H for f, p, H in zip(fns, params, Hs))
+        return (-1j * Ht @ U).reshape(-1)
+
+    sol = solve_ivp(rhs, (t0, t1), np.eye(d, dtype=np.complex128).reshape(-1), method="DOP853", rtol=rtol,
+                    atol=rtol)
+    return sol.y[:, -1].reshape(d, d)
