@@ -432,9 +432,11 @@ void emit_pass(std::ostringstream& o, const jq_plan* plan, const Schedule& s, in
   const int smat_pad = (pd.smat_len + 1) & ~1;
   int nmc = 0;
   for (int ri = pd.rop_begin; ri < pd.rop_end; ++ri) nmc += s.rops[ri].mat_len > 0;
+  // the pass reads `state` and writes `out` (the same buffer for an
+  // in-place pass, another one for the checkpointed reverse pass's recompute)
   o << "extern \"C\" __global__ void __launch_bounds__(" << nthr << ", " << minb << ") @KERNEL@(" << T
-    << "* __restrict__ state, int batch, const " << T << "* __restrict__ bmat, long long bstride, "
-    << "const int* __restrict__ mc) {\n";
+    << "* state, int batch, const " << T << "* __restrict__ bmat, long long bstride, "
+    << "const int* __restrict__ mc, " << T << "* out) {\n";
   // nbuf tile buffers: the next nbuf - 1 tiles stream in (cp.async) while
   // this one is computed
   const int nbuf = jit_bufs();
@@ -517,7 +519,7 @@ void emit_pass(std::ostringstream& o, const jq_plan* plan, const Schedule& s, in
   o << "    cur = cur + 1 == " << nbuf << " ? 0 : cur + 1;\n";
   o << "    cp_commit();\n";
   o << "    const long long inst = tile >> " << (nb - t) << ";\n";
-  o << "    " << T << "* g = gaddr(tile);\n";
+  o << "    " << T << "* g = out + (gaddr(tile) - state);\n";
   // gate matrices of this pass: mc holds (smem offset, block-matrix offset,
   // length) per matrix, so passes that differ only in their gates share code
   o << "    if (inst != last_inst) {\n      const " << T << "* bm = bmat + inst * bstride;\n";
@@ -1655,7 +1657,8 @@ size_t jit_smem(const Schedule& s, int p, int elem) {
 }
 
 int jit_launch(const JitModule& m, const Schedule& s, int p, int n_bits, int sm_count, void* state, int batch,
-               const void* bmat, int64_t bstride, int elem, cudaStream_t st) {
+               const void* bmat, int64_t bstride, int elem, cudaStream_t st, void* out) {
+  if (!out) out = state;
   CUfunction f = static_cast<CUfunction>(m.fn[p]);
   const PassDesc& pd = s.passes[p];
   const int threads = 1 << (pd.t - s.reg_bits);
@@ -1668,7 +1671,7 @@ int jit_launch(const JitModule& m, const Schedule& s, int p, int n_bits, int sm_
   const unsigned grid = static_cast<unsigned>(std::max<int64_t>(1, std::min(ntiles, cap)));
   long long bs = bstride;
   const int32_t* mc = static_cast<const int32_t*>(m.mc) + m.mc_off[p];
-  void* args[] = {&state, &batch, const_cast<void**>(&bmat), &bs, &mc};
+  void* args[] = {&state, &batch, const_cast<void**>(&bmat), &bs, &mc, &out};
   if (g_drv.launch(f, grid, 1, 1, threads, 1, 1, static_cast<unsigned>(smem), reinterpret_cast<CUstream>(st), args,
                    nullptr) != CUDA_SUCCESS) {
     set_error("cuLaunchKernel failed for a specialised pass");

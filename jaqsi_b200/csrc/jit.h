@@ -31,8 +31,9 @@ int jit_build(const jq_plan* plan, const Schedule& s, JitModule* out);
 void jit_free(JitModule* m);
 size_t jit_smem(const Schedule& s, int p, int elem);
 int jit_bufs();
+// One forward pass reading `state` and writing `out` (NULL: in place).
 int jit_launch(const JitModule& m, const Schedule& s, int p, int n_bits, int sm_count, void* state, int batch,
-               const void* bmat, int64_t bstride, int elem, cudaStream_t st);
+               const void* bmat, int64_t bstride, int elem, cudaStream_t st, void* out = nullptr);
 
 size_t jit_adj_smem(const Schedule& s, int p, int elem);
 // One checkpointed reverse pass: xin is the state before the pass (read

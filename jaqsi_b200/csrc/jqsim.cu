@@ -2512,6 +2512,14 @@ int backward_impl(const jq_plan* plan, int batch, const double* angles, const vo
     // states before passes p0..p1-1: seg[j] = state before pass p0 + j
     JQ_CUDA(cudaMemcpyAsync(seg(0), ckpt(c), sizeof(C) * elems * batch, cudaMemcpyDeviceToDevice, st));
     for (int64_t j = 0; j + 1 < p1 - p0; ++j) {
+      const size_t pj = static_cast<size_t>(p0 + j);
+      if (jm && pj < jm->fn.size() && jm->fn[pj]) {
+        // the specialised pass reads seg(j) and writes seg(j + 1): no copy
+        if ((rc = jit_launch(*jm, sch, static_cast<int>(pj), plan->n_bits, sm_count(), seg(j), batch, bmat,
+                             plan->bmat_stride, static_cast<int>(sizeof(C)), st, seg(j + 1))))
+          return rc;
+        continue;
+      }
       JQ_CUDA(cudaMemcpyAsync(seg(j + 1), seg(j), sizeof(C) * elems * batch, cudaMemcpyDeviceToDevice, st));
       if ((rc = run_passes<R>(plan, sch, sops, T->fwd_steps, T->fwd_rops, T, seg(j + 1), batch, bmat, p0 + j, p0 + j + 1, st, jm))) return rc;
     }
