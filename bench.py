@@ -979,6 +979,8 @@ def main():
     ap.add_argument("--shift-sample", type=int, default=24,
                     help="instances whose parameter-shift baseline is timed and scaled")
     ap.add_argument("--dm-sets", type=int, default=64, help="parameter sets of the noisy density-matrix leg")
+    ap.add_argument("--only-dm", action="store_true",
+                    help="run only the noisy density-matrix leg on one GPU and print its JSON (profiling runs)")
     args = ap.parse_args()
     if args.impl == "reference":
         return reference_arm(args)
@@ -988,6 +990,13 @@ def main():
         torch.cuda.set_device(0)
         args.shift_sample = min(args.shift_sample, args.batch_instances)
         print(json.dumps(batched_adjoint_leg(args, torch.device("cuda", 0), args.steps, args.warmup)))
+        return 0
+    if args.only_dm:
+        import torch
+
+        torch.cuda.set_device(0)
+        print(json.dumps(noisy_dm_leg(torch.device("cuda", 0), args.dm_sets, 1, not args.no_cpu, _peaks()[0]),
+                         default=float))
         return 0
     return ours_arm(args)
 
