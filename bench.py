@@ -749,7 +749,7 @@ def adjoint_20q_leg(dev, steps, cpu, hbm_peak, l2_gbs):
     return out
 
 
-def noisy_dm_leg(dev, sets, steps, cpu, hbm_peak, world=1, max_over_ranks=None):
+def noisy_dm_leg(dev, sets, steps, cpu, hbm_peak, world=1, max_over_ranks=None, dtypes=("c128", "c64")):
     """12-qubit density matrix, 20 layers of RX/RY/RZ on every wire + CX
     ring, DepolarizingChannel(0.01) then AmplitudeDamping(0.005) on every
     wire each gate touches, sum_i <Z_i>: forward + checkpointed reverse
@@ -780,6 +780,8 @@ def noisy_dm_leg(dev, sets, steps, cpu, hbm_peak, world=1, max_over_ranks=None):
                     "device-only (jq_forward + jq_backward, one parameter set)"}
     evs = {}
     for dt, name in ((torch.complex128, "c128"), (torch.complex64, "c64")):
+        if name not in dtypes:
+            continue
         p = torch.tensor(ang, requires_grad=True)
         holder = {}
 
@@ -832,6 +834,8 @@ def noisy_dm_leg(dev, sets, steps, cpu, hbm_peak, world=1, max_over_ranks=None):
                                          f"for parameter set 0, OpenMP C, scaled x{sets}; forward only (the "
                                          f"reference has no reverse pass for noisy circuits)"}
     return out
+
+
 def ours_arm(args):
     import torch
     import torch.distributed as dist
@@ -979,6 +983,8 @@ def main():
     ap.add_argument("--shift-sample", type=int, default=24,
                     help="instances whose parameter-shift baseline is timed and scaled")
     ap.add_argument("--dm-sets", type=int, default=64, help="parameter sets of the noisy density-matrix leg")
+    ap.add_argument("--dm-dtypes", nargs="+", default=["c128", "c64"], choices=["c128", "c64"],
+                    help="dtypes of the noisy density-matrix leg with --only-dm")
     ap.add_argument("--only-dm", action="store_true",
                     help="run only the noisy density-matrix leg on one GPU and print its JSON (profiling runs)")
     args = ap.parse_args()
@@ -995,8 +1001,8 @@ def main():
         import torch
 
         torch.cuda.set_device(0)
-        print(json.dumps(noisy_dm_leg(torch.device("cuda", 0), args.dm_sets, 1, not args.no_cpu, _peaks()[0]),
-                         default=float))
+        print(json.dumps(noisy_dm_leg(torch.device("cuda", 0), args.dm_sets, 1, not args.no_cpu, _peaks()[0],
+                                      dtypes=args.dm_dtypes), default=float))
         return 0
     return ours_arm(args)
 
