@@ -34,7 +34,32 @@ struct BPlan {
   int32_t n, nblocks, blk_off;     // BBlock and DevBlock rows [blk_off, blk_off + nblocks)
   int32_t n_angles, obs_off, n_obs;
   int32_t bmat_stride, grad_stride;
-  int32_t cls;                     // 0 warp, 1 cta, 2 tile
+  int32_t cls;                     // 0 warp, 1 cta, 2 tile, 3 cluster
+  int32_t stg_off, n_stg;          // register-stage program (cluster class): RStage rows
+};
+
+// Register-stage program of a cluster-class instance (complex64, 16
+// amplitudes a thread).  A stage loads, for every thread, the 16 amplitudes
+// whose 4 register bits vary and whose other index bits are the thread's
+// index T (over the whole cluster) deposited at tpos[], applies its ops in
+// registers and stores them back; one shared-memory sweep per stage instead
+// of one per block.
+enum { RO_DENSE1 = 0, RO_DENSE2 = 1, RO_DIAG = 2, RO_PERM1 = 3, RO_PERM2 = 4 };
+
+struct RStage {
+  int32_t op_begin, op_end;  // ROp rows
+  int32_t dist;              // a register bit is a rank bit: the stage reads other CTAs' slices
+  uint8_t rpos[4];           // flat index bit of register bit q
+  uint8_t tpos[20];          // flat index bit of thread-index bit i (n - 4 used)
+};
+
+struct ROp {
+  int32_t kind, nt;
+  int32_t q0, q1;            // register bits of target 0 (matrix MSB) and target 1
+  uint32_t crm;              // controls on register bits (mask over register bits)
+  uint32_t ctm;              // controls on thread bits (mask over flat index bits)
+  int32_t mat_off, grad_off;
+  int32_t perm, iperm;       // RO_PERM*: output row r takes input row (perm >> 2r) & 3; iperm inverts it
 };
 
 struct BInst {
@@ -513,6 +538,8 @@ struct ClusterArgs {
   BatchArgs a;
   int lbits;          // L: local index bits per CTA
   void* xs_ws;        // per CTA: 2 * 2^L run-dtype complex exchange scratch
+  const RStage* stg;  // register-stage programs (k_batch_rs)
+  const ROp* rop;
 };
 
 __device__ __forceinline__ bool bdist(const BBlock& B, int lbits) {
@@ -891,6 +918,513 @@ __global__ void __launch_bounds__(512, 1) k_batch_cluster(ClusterArgs ca) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// register-stage cluster class (complex64): the same instances as
+// k_batch_cluster, one shared-memory sweep per stage of up to 4 register
+// bits (RStage) instead of one per block.  psi and lambda slices are stored
+// under rs_swz (an XOR-linear involution of the local offset that folds the
+// higher bits into the four bank-group bits), so the 16 lanes of a
+// shared-memory wavefront, which the stage builder places on local bits of
+// distinct residues mod 4, hit distinct banks.  A thread owns its 16
+// amplitudes for the whole stage, so a stage updates them in place; a stage
+// with a rank bit among its register bits reads and writes other CTAs'
+// slices through distributed shared memory between two cluster barriers.
+// Block cotangents are reduced per op: a warp reduce-scatter, then float
+// atomics into this CTA's shared accumulator, summed over the cluster once
+// per instance.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t rs_swz(uint32_t a) { return a ^ (((a >> 4) ^ (a >> 8) ^ (a >> 12)) & 15u); }
+
+// Packed complex64 products in the two-accumulator form: with broadcast
+// pairs mr = (re, re), mi = (im, im) of each matrix entry, p = sum mr * x and
+// q = sum mi * x, the product is (p.x - q.y, p.y + q.x) (conj entries:
+// (p.x + q.y, p.y - q.x)).
+__device__ __forceinline__ void rs_coef(float2 m, float2& r, float2& i) {
+  r = make_float2(m.x, m.x);
+  i = make_float2(m.y, m.y);
+}
+__device__ __forceinline__ float2 rs_fin(float2 p, float2 q) { return make_float2(p.x - q.y, p.y + q.x); }
+__device__ __forceinline__ float2 rs_finc(float2 p, float2 q) { return make_float2(p.x + q.y, p.y - q.x); }
+// m x + n y
+__device__ __forceinline__ float2 rs_dot(float2 mr, float2 mi, float2 nr, float2 ni, float2 x, float2 y) {
+  return rs_fin(__ffma2_rn(nr, y, __fmul2_rn(mr, x)), __ffma2_rn(ni, y, __fmul2_rn(mi, x)));
+}
+// conj(m) x + conj(n) y
+__device__ __forceinline__ float2 rs_dotc(float2 mr, float2 mi, float2 nr, float2 ni, float2 x, float2 y) {
+  return rs_finc(__ffma2_rn(nr, y, __fmul2_rn(mr, x)), __ffma2_rn(ni, y, __fmul2_rn(mi, x)));
+}
+
+// Reduce 8 per-thread float partials over the warp and add them to dst[0..7].
+__device__ __forceinline__ void rs_flush8(float (&g)[8], float* dst, unsigned lane) {
+  WarpRS<16, 8, float>::run(g, lane);
+  if ((lane & 3u) == 0) atomicAdd(dst + (lane >> 2), g[0]);
+}
+
+__device__ __forceinline__ float2 rs_sel4(float2 a0, float2 a1, float2 a2, float2 a3, int k) {
+  const float2 lo = (k & 1) ? a1 : a0, hi = (k & 1) ? a3 : a2;
+  return (k & 2) ? hi : lo;
+}
+
+// forward one-target dense block on register bit Q
+template <int Q, bool CTRL>
+__device__ __forceinline__ void rs_d1(float2 (&v)[16], const float2* M, uint32_t crm, bool tp) {
+  float2 ar, ai, br, bi, cr, ci, dr, di;
+  rs_coef(M[0], ar, ai);
+  rs_coef(M[1], br, bi);
+  rs_coef(M[2], cr, ci);
+  rs_coef(M[3], dr, di);
+#pragma unroll
+  for (int j = 0; j < 16; ++j) {
+    if (j & (1 << Q)) continue;
+    const int k = j | (1 << Q);
+    const float2 x = v[j], y = v[k];
+    const float2 nx = rs_dot(ar, ai, br, bi, x, y);
+    const float2 ny = rs_dot(cr, ci, dr, di, x, y);
+    if (CTRL) {
+      const bool on = tp && ((static_cast<uint32_t>(j) & crm) == crm);
+      v[j] = on ? nx : x;
+      v[k] = on ? ny : y;
+    } else {
+      v[j] = nx;
+      v[k] = ny;
+    }
+  }
+}
+
+// reverse one-target dense block: psi <- G^dagger psi, cotangent += lam psi^dagger,
+// lam <- G^dagger lam
+template <int Q>
+__device__ __forceinline__ void rs_d1_adj(float2 (&vp)[16], float2 (&vl)[16], const float2* M, uint32_t crm, bool tp,
+                                          float* dst, unsigned lane) {
+  // G^dagger = [[conj m00, conj m10], [conj m01, conj m11]]
+  float2 ar, ai, br, bi, cr, ci, dr, di;
+  rs_coef(M[0], ar, ai);
+  rs_coef(M[2], br, bi);
+  rs_coef(M[1], cr, ci);
+  rs_coef(M[3], dr, di);
+  float g[8];
+#pragma unroll
+  for (int e = 0; e < 8; ++e) g[e] = 0.f;
+#pragma unroll
+  for (int j = 0; j < 16; ++j) {
+    if (j & (1 << Q)) continue;
+    const int k = j | (1 << Q);
+    if (!(tp && ((static_cast<uint32_t>(j) & crm) == crm))) continue;
+    const float2 x = vp[j], y = vp[k];
+    const float2 p0 = rs_dotc(ar, ai, br, bi, x, y);
+    const float2 p1 = rs_dotc(cr, ci, dr, di, x, y);
+    const float2 u = vl[j], w = vl[k];
+    vp[j] = p0;
+    vp[k] = p1;
+    acc_lconjp(g[0], g[1], u, p0);
+    acc_lconjp(g[2], g[3], u, p1);
+    acc_lconjp(g[4], g[5], w, p0);
+    acc_lconjp(g[6], g[7], w, p1);
+    vl[j] = rs_dotc(ar, ai, br, bi, u, w);
+    vl[k] = rs_dotc(cr, ci, dr, di, u, w);
+  }
+  if (dst) rs_flush8(g, dst, lane);
+}
+
+// forward two-target dense block on register bits (Q0 = matrix MSB, Q1)
+template <int Q0, int Q1>
+__device__ __forceinline__ void rs_d2(float2 (&v)[16], const float2* M, uint32_t crm, bool tp) {
+#pragma unroll
+  for (int j = 0; j < 16; ++j) {
+    if ((j >> Q0) & 1 || (j >> Q1) & 1) continue;
+    if (!(tp && ((static_cast<uint32_t>(j) & crm) == crm))) continue;
+    const int id[4] = {j, j | (1 << Q1), j | (1 << Q0), j | (1 << Q0) | (1 << Q1)};
+    float2 a[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) a[c] = v[id[c]];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      float2 mr, mi;
+      rs_coef(M[4 * r], mr, mi);
+      float2 p = __fmul2_rn(mr, a[0]), q = __fmul2_rn(mi, a[0]);
+#pragma unroll
+      for (int c = 1; c < 4; ++c) {
+        rs_coef(M[4 * r + c], mr, mi);
+        p = __ffma2_rn(mr, a[c], p);
+        q = __ffma2_rn(mi, a[c], q);
+      }
+      v[id[r]] = rs_fin(p, q);
+    }
+  }
+}
+
+// G^dagger applied to the group of v at base j (rows r = sum_q conj M[4q + r] a_q)
+template <int Q0, int Q1>
+__device__ __forceinline__ void rs_d2h(float2 (&v)[16], const float2* M, int j) {
+  const int id[4] = {j, j | (1 << Q1), j | (1 << Q0), j | (1 << Q0) | (1 << Q1)};
+  float2 a[4];
+#pragma unroll
+  for (int c = 0; c < 4; ++c) a[c] = v[id[c]];
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    float2 mr, mi;
+    rs_coef(M[r], mr, mi);
+    float2 p = __fmul2_rn(mr, a[0]), q = __fmul2_rn(mi, a[0]);
+#pragma unroll
+    for (int c = 1; c < 4; ++c) {
+      rs_coef(M[4 * c + r], mr, mi);
+      p = __ffma2_rn(mr, a[c], p);
+      q = __ffma2_rn(mi, a[c], q);
+    }
+    v[id[r]] = rs_finc(p, q);
+  }
+}
+
+template <int Q0, int Q1>
+__device__ __forceinline__ void rs_d2_adj(float2 (&vp)[16], float2 (&vl)[16], const float2* M, uint32_t crm, bool tp,
+                                          float* dst, unsigned lane) {
+#pragma unroll
+  for (int j = 0; j < 16; ++j) {
+    if ((j >> Q0) & 1 || (j >> Q1) & 1) continue;
+    if (tp && ((static_cast<uint32_t>(j) & crm) == crm)) rs_d2h<Q0, Q1>(vp, M, j);
+  }
+  if (dst) {
+    // cotangent row r: lam_r (before its update) times conj of the new psi
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      float g[8];
+#pragma unroll
+      for (int e = 0; e < 8; ++e) g[e] = 0.f;
+#pragma unroll
+      for (int j = 0; j < 16; ++j) {
+        if ((j >> Q0) & 1 || (j >> Q1) & 1) continue;
+        if (!(tp && ((static_cast<uint32_t>(j) & crm) == crm))) continue;
+        const int id[4] = {j, j | (1 << Q1), j | (1 << Q0), j | (1 << Q0) | (1 << Q1)};
+#pragma unroll
+        for (int q = 0; q < 4; ++q) acc_lconjp(g[2 * q], g[2 * q + 1], vl[id[r]], vp[id[q]]);
+      }
+      rs_flush8(g, dst + 8 * r, lane);
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < 16; ++j) {
+    if ((j >> Q0) & 1 || (j >> Q1) & 1) continue;
+    if (tp && ((static_cast<uint32_t>(j) & crm) == crm)) rs_d2h<Q0, Q1>(vl, M, j);
+  }
+}
+
+__device__ __forceinline__ int rs_drow(int j, const ROp& op) {
+  return op.nt == 1 ? ((j >> op.q0) & 1) : ((((j >> op.q0) & 1) << 1) | ((j >> op.q1) & 1));
+}
+
+__device__ __forceinline__ void rs_diag(float2 (&v)[16], const float2* M, const ROp& op, bool tp) {
+#pragma unroll
+  for (int j = 0; j < 16; ++j) {
+    if (!(tp && ((static_cast<uint32_t>(j) & op.crm) == op.crm))) continue;
+    float2 mr, mi;
+    rs_coef(M[rs_drow(j, op)], mr, mi);
+    v[j] = rs_fin(__fmul2_rn(mr, v[j]), __fmul2_rn(mi, v[j]));
+  }
+}
+
+__device__ __forceinline__ void rs_diag_adj(float2 (&vp)[16], float2 (&vl)[16], const float2* M, const ROp& op,
+                                            bool tp, float* dst, unsigned lane) {
+  float g[8];
+#pragma unroll
+  for (int e = 0; e < 8; ++e) g[e] = 0.f;
+#pragma unroll
+  for (int j = 0; j < 16; ++j) {
+    if (!(tp && ((static_cast<uint32_t>(j) & op.crm) == op.crm))) continue;
+    const int r = rs_drow(j, op);
+    float2 mr, mi;
+    rs_coef(M[r], mr, mi);
+    const float2 p = rs_finc(__fmul2_rn(mr, vp[j]), __fmul2_rn(mi, vp[j]));
+    const float2 l = vl[j];
+    vp[j] = p;
+    vl[j] = rs_finc(__fmul2_rn(mr, l), __fmul2_rn(mi, l));
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+      if (q == r) acc_lconjp(g[2 * q], g[2 * q + 1], l, p);
+  }
+  if (dst) rs_flush8(g, dst, lane);
+}
+
+// one-target permutation (X on register bit Q); its own inverse
+template <int Q>
+__device__ __forceinline__ void rs_p1(float2 (&v)[16], uint32_t crm, bool tp) {
+#pragma unroll
+  for (int j = 0; j < 16; ++j) {
+    if (j & (1 << Q)) continue;
+    const int k = j | (1 << Q);
+    const bool on = tp && ((static_cast<uint32_t>(j) & crm) == crm);
+    const float2 x = v[j], y = v[k];
+    v[j] = on ? y : x;
+    v[k] = on ? x : y;
+  }
+}
+
+// two-target permutation: output row r takes input row (perm >> 2r) & 3
+template <int Q0, int Q1>
+__device__ __forceinline__ void rs_p2(float2 (&v)[16], int perm, uint32_t crm, bool tp) {
+#pragma unroll
+  for (int j = 0; j < 16; ++j) {
+    if ((j >> Q0) & 1 || (j >> Q1) & 1) continue;
+    if (!(tp && ((static_cast<uint32_t>(j) & crm) == crm))) continue;
+    const int id[4] = {j, j | (1 << Q1), j | (1 << Q0), j | (1 << Q0) | (1 << Q1)};
+    const float2 a0 = v[id[0]], a1 = v[id[1]], a2 = v[id[2]], a3 = v[id[3]];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) v[id[r]] = rs_sel4(a0, a1, a2, a3, (perm >> (2 * r)) & 3);
+  }
+}
+
+// Dispatch over the (Q0, Q1) pairs of distinct register bits.
+#define JQ_RS_PAIRS(F, ...)                                     \
+  switch (op.q0 * 4 + op.q1) {                                  \
+    case 1: F<0, 1>(__VA_ARGS__); break;                        \
+    case 2: F<0, 2>(__VA_ARGS__); break;                        \
+    case 3: F<0, 3>(__VA_ARGS__); break;                        \
+    case 4: F<1, 0>(__VA_ARGS__); break;                        \
+    case 6: F<1, 2>(__VA_ARGS__); break;                        \
+    case 7: F<1, 3>(__VA_ARGS__); break;                        \
+    case 8: F<2, 0>(__VA_ARGS__); break;                        \
+    case 9: F<2, 1>(__VA_ARGS__); break;                        \
+    case 11: F<2, 3>(__VA_ARGS__); break;                       \
+    case 12: F<3, 0>(__VA_ARGS__); break;                       \
+    case 13: F<3, 1>(__VA_ARGS__); break;                       \
+    case 14: F<3, 2>(__VA_ARGS__); break;                       \
+    default: break;                                             \
+  }
+#define JQ_RS_ONE(F, ...)                                       \
+  switch (op.q0) {                                              \
+    case 0: F<0>(__VA_ARGS__); break;                           \
+    case 1: F<1>(__VA_ARGS__); break;                           \
+    case 2: F<2>(__VA_ARGS__); break;                           \
+    default: F<3>(__VA_ARGS__); break;                          \
+  }
+
+__device__ __forceinline__ void rs_fwd_op(float2 (&v)[16], const ROp& op, const float2* bm, uint32_t g0) {
+  const bool tp = (g0 & op.ctm) == op.ctm;
+  const float2* M = bm + op.mat_off;
+  const uint32_t crm = op.crm;
+  switch (op.kind) {
+    case RO_DENSE1:
+      if (crm == 0 && op.ctm == 0) {
+        switch (op.q0) {
+          case 0: rs_d1<0, false>(v, M, crm, tp); break;
+          case 1: rs_d1<1, false>(v, M, crm, tp); break;
+          case 2: rs_d1<2, false>(v, M, crm, tp); break;
+          default: rs_d1<3, false>(v, M, crm, tp); break;
+        }
+      } else {
+        switch (op.q0) {
+          case 0: rs_d1<0, true>(v, M, crm, tp); break;
+          case 1: rs_d1<1, true>(v, M, crm, tp); break;
+          case 2: rs_d1<2, true>(v, M, crm, tp); break;
+          default: rs_d1<3, true>(v, M, crm, tp); break;
+        }
+      }
+      break;
+    case RO_DENSE2: JQ_RS_PAIRS(rs_d2, v, M, crm, tp) break;
+    case RO_DIAG: rs_diag(v, M, op, tp); break;
+    case RO_PERM1: JQ_RS_ONE(rs_p1, v, crm, tp) break;
+    default: JQ_RS_PAIRS(rs_p2, v, op.perm, crm, tp) break;
+  }
+}
+
+__device__ __forceinline__ void rs_adj_op(float2 (&vp)[16], float2 (&vl)[16], const ROp& op, const float2* bm,
+                                          uint32_t g0, float* acc, unsigned lane) {
+  const bool tp = (g0 & op.ctm) == op.ctm;
+  const float2* M = bm + op.mat_off;
+  const uint32_t crm = op.crm;
+  float* dst = op.grad_off >= 0 ? acc + 2 * op.grad_off : nullptr;
+  switch (op.kind) {
+    case RO_DENSE1: JQ_RS_ONE(rs_d1_adj, vp, vl, M, crm, tp, dst, lane) break;
+    case RO_DENSE2: JQ_RS_PAIRS(rs_d2_adj, vp, vl, M, crm, tp, dst, lane) break;
+    case RO_DIAG: rs_diag_adj(vp, vl, M, op, tp, dst, lane); break;
+    case RO_PERM1:
+      JQ_RS_ONE(rs_p1, vp, crm, tp)
+      JQ_RS_ONE(rs_p1, vl, crm, tp)
+      break;
+    default:
+      JQ_RS_PAIRS(rs_p2, vp, op.iperm, crm, tp)
+      JQ_RS_PAIRS(rs_p2, vl, op.iperm, crm, tp)
+      break;
+  }
+}
+
+// Thread base index of a stage (thread-index bit i at flat bit tpos[i]) and
+// the flat bits of its 4 register bits.
+__device__ __forceinline__ uint32_t rs_base(const RStage* S, uint32_t T, int ntb) {
+  uint32_t g = 0;
+  for (int i = 0; i < ntb; ++i) g |= ((T >> i) & 1u) << S->tpos[i];
+  return g;
+}
+
+template <int J>
+__device__ __forceinline__ uint32_t rs_sel(uint32_t r0, uint32_t r1, uint32_t r2, uint32_t r3) {
+  return ((J & 1) ? r0 : 0u) ^ ((J & 2) ? r1 : 0u) ^ ((J & 4) ? r2 : 0u) ^ ((J & 8) ? r3 : 0u);
+}
+
+// Load / store the 16 amplitudes of a stage: a local stage addresses this
+// CTA's slice (offset = swz(base) ^ swz(register bits)); a distributed one
+// maps every amplitude to the CTA holding it.
+template <bool STORE, int J = 0>
+__device__ __forceinline__ void rs_move_local(float2 (&v)[16], float2* buf, uint32_t base, uint32_t s0, uint32_t s1,
+                                              uint32_t s2, uint32_t s3) {
+  if constexpr (J < 16) {
+    const uint32_t off = base ^ rs_sel<J>(s0, s1, s2, s3);
+    if (STORE) buf[off] = v[J];
+    else v[J] = buf[off];
+    rs_move_local<STORE, J + 1>(v, buf, base, s0, s1, s2, s3);
+  }
+}
+
+template <bool STORE, int J = 0>
+__device__ __forceinline__ void rs_move_dist(cooperative_groups::cluster_group& cl, float2 (&v)[16], float2* buf,
+                                             uint32_t g0, uint32_t r0, uint32_t r1, uint32_t r2, uint32_t r3, int lb) {
+  if constexpr (J < 16) {
+    const uint32_t g = g0 ^ rs_sel<J>(r0, r1, r2, r3);
+    float2* p = cl.map_shared_rank(buf + rs_swz(g & ((1u << lb) - 1u)), g >> lb);
+    if (STORE) *p = v[J];
+    else v[J] = *p;
+    rs_move_dist<STORE, J + 1>(cl, v, buf, g0, r0, r1, r2, r3, lb);
+  }
+}
+
+template <int CL>
+__global__ void __launch_bounds__(512, 1) k_batch_rs(ClusterArgs ca) {
+  namespace cg = cooperative_groups;
+  cg::cluster_group cluster = cg::this_cluster();
+  const BatchArgs& a = ca.a;
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int lb = ca.lbits, nloc = 1 << lb;
+  const uint32_t lmask = static_cast<uint32_t>(nloc) - 1u;
+  const int gs = static_cast<int>(blockDim.x), lt = static_cast<int>(threadIdx.x);
+  const unsigned lane = threadIdx.x & 31u;
+  const uint32_t rank = cluster.block_rank();
+  const uint32_t T = rank * static_cast<uint32_t>(gs) + static_cast<uint32_t>(lt);
+  float2* sp = reinterpret_cast<float2*>(smem);
+  float2* sl = sp + nloc;
+  float2* bm = sl + nloc;                                    // block matrices of the instance
+  float* acc = reinterpret_cast<float*>(bm + a.bmat_slot);   // this CTA's block cotangents
+  double* red = reinterpret_cast<double*>(acc + 2 * a.gacc_slot);
+  double* spart = red + 32;
+  int* snext = reinterpret_cast<int*>(spart + 32);
+  const int64_t cid = blockIdx.x / CL;
+  double2* gacc = a.gacc_ws + cid * a.gacc_slot;
+  const uint32_t gbase = rank << lb;
+  for (;;) {
+    if (rank == 0 && lt == 0) snext[0] = atomicAdd(a.counter, 1);
+    cluster.sync();
+    const int k = *cluster.map_shared_rank(snext, 0);
+    cluster.sync();
+    if (k >= a.n_order) break;
+    const BInst I = a.inst[a.order[k]];
+    const BPlan P = a.plans[I.plan];
+    const double* ang = a.angles + I.angle_off;
+    for (int b = lt; b < P.nblocks; b += gs)
+      prep_block<float>(a.dblk[P.blk_off + b], a.prims, a.ops, ang, nullptr, a.cpool, bm, nullptr);
+    for (int e = lt; e < 2 * P.grad_stride; e += gs) acc[e] = 0.f;
+    for (int j = lt; j < nloc; j += gs) sp[j] = make_float2((gbase | static_cast<uint32_t>(j)) == 0 ? 1.f : 0.f, 0.f);
+    cluster.sync();
+    const RStage* SS = ca.stg + P.stg_off;
+    const ROp* OPS = ca.rop;
+    const int ntb = P.n - 4;
+    // forward
+    for (int s = 0; s < P.n_stg; ++s) {
+      const RStage* S = SS + s;
+      const bool dist = S->dist != 0;
+      const uint32_t g0 = rs_base(S, T, ntb);
+      const uint32_t r0 = 1u << S->rpos[0], r1 = 1u << S->rpos[1], r2 = 1u << S->rpos[2], r3 = 1u << S->rpos[3];
+      float2 v[16];
+      if (dist) {
+        cluster.sync();
+        rs_move_dist<false>(cluster, v, sp, g0, r0, r1, r2, r3, lb);
+      } else {
+        rs_move_local<false>(v, sp, rs_swz(g0 & lmask), rs_swz(r0), rs_swz(r1), rs_swz(r2), rs_swz(r3));
+      }
+      for (int o = S->op_begin; o < S->op_end; ++o) {
+        const ROp op = OPS[o];
+        rs_fwd_op(v, op, bm, g0);
+      }
+      if (dist) {
+        rs_move_dist<true>(cluster, v, sp, g0, r0, r1, r2, r3, lb);
+        cluster.sync();
+      } else {
+        rs_move_local<true>(v, sp, rs_swz(g0 & lmask), rs_swz(r0), rs_swz(r1), rs_swz(r2), rs_swz(r3));
+        __syncthreads();
+      }
+    }
+    cluster.sync();
+    // expectation values (partial sums per CTA, added by rank 0) and the seed of lambda
+    for (int j = lt; j < nloc; j += gs) sl[j] = make_float2(0.f, 0.f);
+    for (int o = 0; o < P.n_obs; ++o) {
+      const DevObs ob = a.obs[P.obs_off + o];
+      const double w = 2.0 * (a.ct ? a.ct[I.out_off + o] : 1.0) * ob.coeff;
+      double part = 0.0;
+      for (int j = lt; j < nloc; j += gs) {
+        const uint32_t g = gbase | rs_swz(static_cast<uint32_t>(j));
+        const uint32_t gx = g ^ static_cast<uint32_t>(ob.x_mask);
+        const double sign = (__popc(gx & static_cast<uint32_t>(ob.z_mask)) & 1) ? -1.0 : 1.0;
+        const double2 v = mul_iy(ob.n_y, to_d2(*cluster.map_shared_rank(sp + rs_swz(gx & lmask), gx >> lb)));
+        const double2 pj = to_d2(sp[j]);
+        part += sign * (pj.x * v.x + pj.y * v.y);
+        const double2 l = to_d2(sl[j]);
+        sl[j] = make_float2(static_cast<float>(l.x + w * sign * v.x), static_cast<float>(l.y + w * sign * v.y));
+      }
+      const double tot = gsum<false>(part, red);
+      if (lt == 0) spart[o] = tot;
+    }
+    cluster.sync();
+    if (rank == 0 && lt < P.n_obs) {
+      double tot = 0.0;
+      for (int r = 0; r < CL; ++r) tot += *cluster.map_shared_rank(spart + lt, r);
+      a.expval[I.out_off + lt] = a.obs[P.obs_off + lt].coeff * tot;
+    }
+    // adjoint: stages in reverse, each stage's ops in reverse
+    for (int s = P.n_stg - 1; s >= 0; --s) {
+      const RStage* S = SS + s;
+      const bool dist = S->dist != 0;
+      const uint32_t g0 = rs_base(S, T, ntb);
+      const uint32_t r0 = 1u << S->rpos[0], r1 = 1u << S->rpos[1], r2 = 1u << S->rpos[2], r3 = 1u << S->rpos[3];
+      float2 vp[16], vl[16];
+      if (dist) {
+        cluster.sync();
+        rs_move_dist<false>(cluster, vp, sp, g0, r0, r1, r2, r3, lb);
+        rs_move_dist<false>(cluster, vl, sl, g0, r0, r1, r2, r3, lb);
+      } else {
+        const uint32_t base = rs_swz(g0 & lmask);
+        rs_move_local<false>(vp, sp, base, rs_swz(r0), rs_swz(r1), rs_swz(r2), rs_swz(r3));
+        rs_move_local<false>(vl, sl, base, rs_swz(r0), rs_swz(r1), rs_swz(r2), rs_swz(r3));
+      }
+      for (int o = S->op_end - 1; o >= S->op_begin; --o) {
+        const ROp op = OPS[o];
+        rs_adj_op(vp, vl, op, bm, g0, acc, lane);
+      }
+      if (dist) {
+        rs_move_dist<true>(cluster, vp, sp, g0, r0, r1, r2, r3, lb);
+        rs_move_dist<true>(cluster, vl, sl, g0, r0, r1, r2, r3, lb);
+        cluster.sync();
+      } else {
+        const uint32_t base = rs_swz(g0 & lmask);
+        rs_move_local<true>(vp, sp, base, rs_swz(r0), rs_swz(r1), rs_swz(r2), rs_swz(r3));
+        rs_move_local<true>(vl, sl, base, rs_swz(r0), rs_swz(r1), rs_swz(r2), rs_swz(r3));
+        __syncthreads();
+      }
+    }
+    cluster.sync();  // every CTA's cotangent contributions are in
+    for (int e = static_cast<int>(rank) * gs + lt; e < P.grad_stride; e += CL * gs) {
+      double re = 0.0, im = 0.0;
+      for (int r = 0; r < CL; ++r) {
+        const float2 c = *reinterpret_cast<const float2*>(cluster.map_shared_rank(acc + 2 * e, r));
+        re += c.x;
+        im += c.y;
+      }
+      gacc[e] = make_double2(re, im);
+    }
+    cluster.sync();
+    for (int b = static_cast<int>(rank) * gs + lt; b < P.nblocks; b += CL * gs)
+      chain_block(a.dblk[P.blk_off + b], a.prims, a.ops, ang, nullptr, a.cpool, gacc, nullptr, a.grad + I.angle_off,
+                  nullptr);
+    cluster.sync();  // the cotangent slots and block matrices are free again
+  }
+}
+
 // gather / scatter between the batch's instance layout and a plan group's
 // dense (instance, entry) layout
 __global__ void k_gather_rows(const double* src, const int64_t* src_off, int rows, int width, double* dst) {
@@ -930,6 +1464,8 @@ struct jq_batch {
   std::vector<jq::DevOp> ops;
   std::vector<double> cpool;
   std::vector<jq::DevObs> obs;
+  std::vector<jq::RStage> rstg;  // register-stage programs of the cluster-class plans
+  std::vector<jq::ROp> rop;
   std::vector<int> n_of_plan;   // qubit count per plan
   // configuration (autotuned)
   jq_batch_config cfg{};
@@ -942,6 +1478,8 @@ struct jq_batch {
   void* d_ops = nullptr;
   void* d_cpool = nullptr;
   void* d_obs = nullptr;
+  void* d_rstg = nullptr;
+  void* d_rop = nullptr;
   void* d_order = nullptr;     // warp-class order then cta-class order
   void* d_tile_off = nullptr;  // per tile group: angle offsets then output offsets of its instances
   // classes under the current configuration
@@ -983,6 +1521,112 @@ int64_t even(int64_t x) { return (x + 1) & ~static_cast<int64_t>(1); }
 
 int64_t plan_cost(const jq_batch* b, int p) {
   return (static_cast<int64_t>(1) << b->n_of_plan[p]) * std::max(1, b->bplans[p].nblocks);
+}
+
+// Register-stage program of one cluster-class plan (n qubits, lb local bits,
+// 16 amplitudes a thread).  Blocks join the current stage greedily in
+// program order while their targets fit in 4 register bits; a block that
+// does not fit, or that shares a bit (target or control) with a block
+// already deferred, is deferred, so every block still follows the blocks it
+// does not commute with.  Free register slots take the highest free local
+// bits.  Thread-index bits: the four lowest take local positions of distinct
+// residues mod 4 (a 16-lane wavefront then hits 16 bank groups under
+// rs_swz), the other lane bits the next local positions, the CTA-rank bits
+// of the thread index what is left, rank positions last (a stage without a
+// rank register bit therefore stays inside each CTA's slice).
+void build_rstages(const BBlock* bb, int nblocks, int n, int lb, std::vector<RStage>* stg, std::vector<ROp>* rops) {
+  std::vector<int> rem(nblocks);
+  for (int i = 0; i < nblocks; ++i) rem[i] = i;
+  while (!rem.empty()) {
+    uint32_t R = 0, blocked = 0;
+    std::vector<int> members;
+    for (int o : rem) {
+      const BBlock& B = bb[o];
+      uint32_t tg = 1u << B.tb0;
+      if (B.nt == 2) tg |= 1u << B.tb1;
+      const uint32_t all = tg | B.cmask;
+      if (all & blocked) {
+        blocked |= all;
+        continue;
+      }
+      if (__builtin_popcount(R | tg) <= 4) {
+        R |= tg;
+        members.push_back(o);
+      } else {
+        blocked |= all;
+      }
+    }
+    for (int pos = lb - 1; pos >= 0 && __builtin_popcount(R) < 4; --pos) R |= 1u << pos;
+    RStage st;
+    std::memset(&st, 0, sizeof(st));
+    int rix[32];
+    int nr = 0;
+    for (int pos = 0; pos < 32; ++pos) rix[pos] = -1;
+    for (int pos = 0; pos < n; ++pos)
+      if (R >> pos & 1u) {
+        st.rpos[nr] = static_cast<uint8_t>(pos);
+        rix[pos] = nr++;
+      }
+    std::vector<int> first, rest;
+    uint32_t classes = 0;
+    for (int pos = 0; pos < lb; ++pos) {
+      if (R >> pos & 1u) continue;
+      const uint32_t cb = 1u << (pos % 4);
+      if (first.size() < 4 && !(classes & cb)) {
+        classes |= cb;
+        first.push_back(pos);
+      } else {
+        rest.push_back(pos);
+      }
+    }
+    first.insert(first.end(), rest.begin(), rest.end());
+    for (int pos = lb; pos < n; ++pos)
+      if (!(R >> pos & 1u)) first.push_back(pos);
+    for (size_t i = 0; i < first.size(); ++i) st.tpos[i] = static_cast<uint8_t>(first[i]);
+    st.dist = (R >> lb) != 0 ? 1 : 0;
+    st.op_begin = static_cast<int32_t>(rops->size());
+    for (int o : members) {
+      const BBlock& B = bb[o];
+      if (B.kind == BK_PERM && B.nt == 1 && (B.perm & 3) == 0) continue;  // identity
+      ROp r;
+      std::memset(&r, 0, sizeof(r));
+      r.nt = B.nt;
+      if (B.kind == BK_DENSE) r.kind = B.nt == 1 ? RO_DENSE1 : RO_DENSE2;
+      else if (B.kind == BK_DIAG) r.kind = RO_DIAG;
+      else r.kind = B.nt == 1 ? RO_PERM1 : RO_PERM2;
+      r.q0 = rix[B.tb0];
+      r.q1 = B.nt == 2 ? rix[B.tb1] : 0;
+      for (int pos = 0; pos < n; ++pos) {
+        if (!(B.cmask >> pos & 1u)) continue;
+        if (rix[pos] >= 0) r.crm |= 1u << rix[pos];
+        else r.ctm |= 1u << pos;
+      }
+      r.mat_off = B.mat_off;
+      r.grad_off = B.grad_off;
+      r.perm = B.perm;
+      if (B.nt == 2)
+        for (int q = 0; q < 4; ++q) r.iperm |= q << (2 * ((B.perm >> (2 * q)) & 3));
+      rops->push_back(r);
+    }
+    st.op_end = static_cast<int32_t>(rops->size());
+    stg->push_back(st);
+    std::vector<int> left;
+    for (int o : rem)
+      if (std::find(members.begin(), members.end(), o) == members.end()) left.push_back(o);
+    rem.swap(left);
+  }
+}
+
+// The register-stage cluster kernel runs a cluster launch when the batch is
+// complex64, a CTA holds 16 amplitudes a thread (cta_threads = 2^(L - 4)),
+// its shared memory also takes the per-CTA cotangent accumulators, and
+// JQ_BATCH_RS is not 0.
+bool batch_rs_ok(const jq_batch* b, int elem) {
+  if (const char* e = std::getenv("JQ_BATCH_RS"))
+    if (std::atoi(e) == 0) return false;
+  const int lb = b->cfg.cta_max_qubits;
+  if (elem != 8 || lb < 8 || lb > 16 || b->cfg.cta_threads != (1 << (lb - 4))) return false;
+  return batch_smem(lb, 1, elem, b->bs_cl) + static_cast<size_t>(b->gacc_slot) * 8 <= 227 * 1024;
 }
 
 // Which class each plan runs in under the configuration.
@@ -1122,6 +1766,26 @@ int batch_classify(jq_batch* b, bool dry) {
   JQ_CUDA(cudaMemcpy(b->d_order, order.data(), order.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
   JQ_CUDA(cudaMalloc(&b->d_tile_off, toff.size() * sizeof(int64_t)));
   JQ_CUDA(cudaMemcpy(b->d_tile_off, toff.data(), toff.size() * sizeof(int64_t), cudaMemcpyHostToDevice));
+  // register-stage programs of the cluster class (they depend on the local bits L)
+  b->rstg.clear();
+  b->rop.clear();
+  for (size_t p = 0; p < b->plans.size(); ++p) {
+    BPlan& bp = b->bplans[p];
+    bp.stg_off = bp.n_stg = 0;
+    if (cls[p] != 3) continue;
+    bp.stg_off = static_cast<int32_t>(b->rstg.size());
+    build_rstages(b->bblk.data() + bp.blk_off, bp.nblocks, b->n_of_plan[p], c.cta_max_qubits, &b->rstg, &b->rop);
+    bp.n_stg = static_cast<int32_t>(b->rstg.size()) - bp.stg_off;
+  }
+  if (b->d_rstg) cudaFree(b->d_rstg);
+  if (b->d_rop) cudaFree(b->d_rop);
+  b->d_rstg = b->d_rop = nullptr;
+  JQ_CUDA(cudaMalloc(&b->d_rstg, std::max<size_t>(1, b->rstg.size()) * sizeof(RStage)));
+  JQ_CUDA(cudaMalloc(&b->d_rop, std::max<size_t>(1, b->rop.size()) * sizeof(ROp)));
+  if (!b->rstg.empty())
+    JQ_CUDA(cudaMemcpy(b->d_rstg, b->rstg.data(), b->rstg.size() * sizeof(RStage), cudaMemcpyHostToDevice));
+  if (!b->rop.empty())
+    JQ_CUDA(cudaMemcpy(b->d_rop, b->rop.data(), b->rop.size() * sizeof(ROp), cudaMemcpyHostToDevice));
   JQ_CUDA(cudaMemcpy(b->d_plans, b->bplans.data(), b->bplans.size() * sizeof(BPlan), cudaMemcpyHostToDevice));
   // workspace: counters, per-slot block matrices and cotangents, tile groups
   int64_t bs = 1, gsl = 1;
@@ -1251,9 +1915,17 @@ int batch_launch_cluster(jq_batch* b, int ci, const double* angles, const double
   a.counter = reinterpret_cast<int*>(w + b->ws_counter) + 2 + ci;
   ca.lbits = lbits;
   ca.xs_ws = w + b->ws_cl_xs + static_cast<size_t>(ci) * b->sm_count * 2 * (static_cast<size_t>(1) << lbits) * elem;
+  ca.stg = static_cast<const RStage*>(b->d_rstg);
+  ca.rop = static_cast<const ROp*>(b->d_rop);
   const int threads = b->cfg.cta_threads;
-  const size_t smem = batch_smem(lbits, 1, elem, a.bmat_slot);
+  size_t smem = batch_smem(lbits, 1, elem, a.bmat_slot);
   auto kern = k_batch_cluster<R, CL>;
+  if constexpr (std::is_same<R, float>::value) {
+    if (batch_rs_ok(b, elem)) {
+      kern = k_batch_rs<CL>;
+      smem += static_cast<size_t>(a.gacc_slot) * 8;
+    }
+  }
   JQ_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
   cudaLaunchConfig_t cfg = {};
   cudaLaunchAttribute attr[1];

@@ -3056,7 +3056,7 @@ int jq_batch_free(jq_batch* b) {
   if (!b) return JQ_OK;
   if (b->graph) cudaGraphExecDestroy(b->graph);
   void* bufs[] = {b->d_plans, b->d_inst, b->d_bblk, b->d_dblk, b->d_prims, b->d_ops, b->d_cpool, b->d_obs,
-                  b->d_order, b->d_tile_off};
+                  b->d_order, b->d_tile_off, b->d_rstg, b->d_rop};
   for (void* p : bufs)
     if (p) cudaFree(p);
   for (int i = 0; i < 5; ++i)

@@ -132,3 +132,34 @@ def test_batch_cluster_class_all_cluster_sizes():
                                                  cta_threads=threads, cluster_bits=3))
             assert bg.classes["cluster"] == 18, bg.classes
             _check(bg, refs, np.ones(bg.n_obs_total), TOL[dtype])
+
+
+def test_batch_register_stage_cluster_random_gates():
+    """Random circuits over the gate library (one- and two-target dense,
+    diagonal and permutation blocks, controls on register and thread bits)
+    at 11-13 qubits with a 10-qubit CTA slice and 64 threads a CTA: the
+    complex64 cluster class then runs as register stages (16 amplitudes a
+    thread), stages with rank bits exchanging through distributed shared
+    memory.  Against the oracle, with cotangent weights."""
+    rng = np.random.default_rng(31)
+    inst, refs = [], []
+    for i in range(15):
+        n = 11 + i % 3
+        params = torch.tensor(rng.uniform(0, 2 * np.pi, 400))
+        with jq.recording() as tape:
+            for w in range(n):
+                jq.H(wires=w)
+            random_circuit(n, 90, np.random.default_rng(3000 + i), params, wide=False)
+            jq.CCX(wires=[n - 1, 0, 5])
+            jq.CSWAP(wires=[1, n - 2, 3])
+        obs = [jq.PauliZ(0), jq.PauliX(n - 1), jq.build_parity_observable([2, n - 3]), jq.PauliY(n // 2)]
+        inst.append((tape, n, obs))
+        refs.append((to_records(tape), n, obs_records(obs)))
+    bg = jq.BatchedGradients(inst, dtype=torch.complex64,
+                             config=dict(warp_max_qubits=0, cta_max_qubits=10, warp_threads=64, cta_threads=64,
+                                         cluster_bits=3))
+    assert bg.classes["cluster"] == 15, bg.classes
+    ct = np.random.default_rng(6).normal(size=bg.n_obs_total)
+    bg.set_cotangents(torch.tensor(ct))
+    _check(bg, refs, ct, 1e-5)
+    _check(bg, refs, ct, 1e-5)
