@@ -46,13 +46,22 @@ struct BPlan {
 // of one per block.
 enum { RO_DENSE1 = 0, RO_DENSE2 = 1, RO_DIAG = 2, RO_PERM1 = 3, RO_PERM2 = 4 };
 
-struct RStage {
-  int32_t op_begin, op_end;  // ROp rows
+struct alignas(16) RStage {
+  int32_t op_begin, op_end;  // RPacked rows
   int32_t dist;              // a register bit is a rank bit: the stage reads other CTAs' slices
-  uint8_t rpos[4];           // flat index bit of register bit q
-  uint8_t tpos[20];          // flat index bit of thread-index bit i (n - 4 used)
+  uint32_t rpos;             // byte q: flat index bit of register bit q
+  uint32_t tpos[5];          // byte i: flat index bit of thread-index bit i (n - 4 used)
+  int32_t pad[3];
 };
 
+// One op of a stage as the device reads it (16 bytes, one vector load):
+// w0 = kind | nt << 3 | q0 << 5 | q1 << 7 | crm << 9 | perm << 13 | iperm << 21
+struct alignas(16) RPacked {
+  uint32_t w0, ctm;
+  int32_t mat_off, grad_off;
+};
+
+// Decoded op.
 struct ROp {
   int32_t kind, nt;
   int32_t q0, q1;            // register bits of target 0 (matrix MSB) and target 1
@@ -61,6 +70,32 @@ struct ROp {
   int32_t mat_off, grad_off;
   int32_t perm, iperm;       // RO_PERM*: output row r takes input row (perm >> 2r) & 3; iperm inverts it
 };
+
+__host__ __device__ inline RPacked rs_pack(const ROp& r) {
+  RPacked p;
+  p.w0 = static_cast<uint32_t>(r.kind) | static_cast<uint32_t>(r.nt) << 3 | static_cast<uint32_t>(r.q0) << 5 |
+         static_cast<uint32_t>(r.q1) << 7 | r.crm << 9 | static_cast<uint32_t>(r.perm & 255) << 13 |
+         static_cast<uint32_t>(r.iperm & 255) << 21;
+  p.ctm = r.ctm;
+  p.mat_off = r.mat_off;
+  p.grad_off = r.grad_off;
+  return p;
+}
+
+__host__ __device__ inline ROp rs_unpack(RPacked p) {
+  ROp r;
+  r.kind = static_cast<int32_t>(p.w0 & 7u);
+  r.nt = static_cast<int32_t>((p.w0 >> 3) & 3u);
+  r.q0 = static_cast<int32_t>((p.w0 >> 5) & 3u);
+  r.q1 = static_cast<int32_t>((p.w0 >> 7) & 3u);
+  r.crm = (p.w0 >> 9) & 15u;
+  r.perm = static_cast<int32_t>((p.w0 >> 13) & 255u);
+  r.iperm = static_cast<int32_t>((p.w0 >> 21) & 255u);
+  r.ctm = p.ctm;
+  r.mat_off = p.mat_off;
+  r.grad_off = p.grad_off;
+  return r;
+}
 
 struct BInst {
   int32_t plan;
@@ -539,7 +574,7 @@ struct ClusterArgs {
   int lbits;          // L: local index bits per CTA
   void* xs_ws;        // per CTA: 2 * 2^L run-dtype complex exchange scratch
   const RStage* stg;  // register-stage programs (k_batch_rs)
-  const ROp* rop;
+  const RPacked* rop;
 };
 
 __device__ __forceinline__ bool bdist(const BBlock& B, int lbits) {
@@ -1247,11 +1282,12 @@ __device__ __forceinline__ void rs_adj_op(float2 (&vp)[16], float2 (&vl)[16], co
   }
 }
 
-// Thread base index of a stage (thread-index bit i at flat bit tpos[i]) and
-// the flat bits of its 4 register bits.
-__device__ __forceinline__ uint32_t rs_base(const RStage* S, uint32_t T, int ntb) {
+// Thread base index of a stage: thread-index bit i at flat bit (byte i of tpos).
+__device__ __forceinline__ uint32_t rs_base(const uint32_t (&tw)[5], uint32_t T, int ntb) {
   uint32_t g = 0;
-  for (int i = 0; i < ntb; ++i) g |= ((T >> i) & 1u) << S->tpos[i];
+#pragma unroll
+  for (int i = 0; i < 20; ++i)
+    if (i < ntb) g |= ((T >> i) & 1u) << ((tw[i >> 2] >> (8 * (i & 3))) & 31u);
   return g;
 }
 
@@ -1260,9 +1296,27 @@ __device__ __forceinline__ uint32_t rs_sel(uint32_t r0, uint32_t r1, uint32_t r2
   return ((J & 1) ? r0 : 0u) ^ ((J & 2) ? r1 : 0u) ^ ((J & 4) ? r2 : 0u) ^ ((J & 8) ? r3 : 0u);
 }
 
-// Load / store the 16 amplitudes of a stage: a local stage addresses this
-// CTA's slice (offset = swz(base) ^ swz(register bits)); a distributed one
-// maps every amplitude to the CTA holding it.
+// Distributed shared memory by address: the 32-bit shared::cluster address
+// of offset `a` (a shared::cta address) in the CTA of cluster rank r, and
+// 8-byte loads / stores through it.
+__device__ __forceinline__ uint32_t rs_mapa(uint32_t a, uint32_t r) {
+  uint32_t out;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(out) : "r"(a), "r"(r));
+  return out;
+}
+__device__ __forceinline__ float2 rs_ldc(uint32_t a) {
+  float2 v;
+  asm volatile("ld.shared::cluster.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "r"(a) : "memory");
+  return v;
+}
+__device__ __forceinline__ void rs_stc(uint32_t a, float2 v) {
+  asm volatile("st.shared::cluster.v2.f32 [%0], {%1, %2};" ::"r"(a), "f"(v.x), "f"(v.y) : "memory");
+}
+
+// Load / store the 16 amplitudes of a stage.  A local stage addresses this
+// CTA's slice: offset = swz(base) ^ swz(register bits), both XOR-linear.  A
+// distributed one splits every index the same way into a local offset and a
+// CTA rank (rank bits of the base XOR the rank bits of the register part).
 template <bool STORE, int J = 0>
 __device__ __forceinline__ void rs_move_local(float2 (&v)[16], float2* buf, uint32_t base, uint32_t s0, uint32_t s1,
                                               uint32_t s2, uint32_t s3) {
@@ -1275,15 +1329,45 @@ __device__ __forceinline__ void rs_move_local(float2 (&v)[16], float2* buf, uint
 }
 
 template <bool STORE, int J = 0>
-__device__ __forceinline__ void rs_move_dist(cooperative_groups::cluster_group& cl, float2 (&v)[16], float2* buf,
-                                             uint32_t g0, uint32_t r0, uint32_t r1, uint32_t r2, uint32_t r3, int lb) {
+__device__ __forceinline__ void rs_move_dist(float2 (&v)[16], uint32_t buf, uint32_t base, uint32_t c0, uint32_t s0,
+                                             uint32_t s1, uint32_t s2, uint32_t s3, uint32_t k0, uint32_t k1,
+                                             uint32_t k2, uint32_t k3) {
   if constexpr (J < 16) {
-    const uint32_t g = g0 ^ rs_sel<J>(r0, r1, r2, r3);
-    float2* p = cl.map_shared_rank(buf + rs_swz(g & ((1u << lb) - 1u)), g >> lb);
-    if (STORE) *p = v[J];
-    else v[J] = *p;
-    rs_move_dist<STORE, J + 1>(cl, v, buf, g0, r0, r1, r2, r3, lb);
+    const uint32_t a = rs_mapa(buf + 8u * (base ^ rs_sel<J>(s0, s1, s2, s3)), c0 ^ rs_sel<J>(k0, k1, k2, k3));
+    if (STORE) rs_stc(a, v[J]);
+    else v[J] = rs_ldc(a);
+    rs_move_dist<STORE, J + 1>(v, buf, base, c0, s0, s1, s2, s3, k0, k1, k2, k3);
   }
+}
+
+// Per-thread addressing of one stage.
+struct RSAddr {
+  uint32_t g0;              // thread base index
+  uint32_t base, c0;        // swz(local part of g0), rank part of g0
+  uint32_t s[4], k[4];      // per register bit: swz(local part), rank part
+};
+
+__device__ __forceinline__ RSAddr rs_addr(const RStage* S, uint32_t T, int ntb, int lb, int& dist, int& ob, int& oe) {
+  const int4 h = *reinterpret_cast<const int4*>(S);
+  const int4 t0 = *(reinterpret_cast<const int4*>(S) + 1);
+  const int4 t1 = *(reinterpret_cast<const int4*>(S) + 2);
+  ob = h.x;
+  oe = h.y;
+  dist = h.z;
+  const uint32_t tw[5] = {static_cast<uint32_t>(t0.x), static_cast<uint32_t>(t0.y), static_cast<uint32_t>(t0.z),
+                          static_cast<uint32_t>(t0.w), static_cast<uint32_t>(t1.x)};
+  RSAddr A;
+  const uint32_t lmask = (1u << lb) - 1u;
+  A.g0 = rs_base(tw, T, ntb);
+  A.base = rs_swz(A.g0 & lmask);
+  A.c0 = A.g0 >> lb;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const uint32_t r = 1u << ((static_cast<uint32_t>(h.w) >> (8 * q)) & 31u);
+    A.s[q] = rs_swz(r & lmask);
+    A.k[q] = r >> lb;
+  }
+  return A;
 }
 
 template <int CL>
@@ -1300,6 +1384,8 @@ __global__ void __launch_bounds__(512, 1) k_batch_rs(ClusterArgs ca) {
   const uint32_t T = rank * static_cast<uint32_t>(gs) + static_cast<uint32_t>(lt);
   float2* sp = reinterpret_cast<float2*>(smem);
   float2* sl = sp + nloc;
+  const uint32_t sp_s = static_cast<uint32_t>(__cvta_generic_to_shared(sp));
+  const uint32_t sl_s = static_cast<uint32_t>(__cvta_generic_to_shared(sl));
   float2* bm = sl + nloc;                                    // block matrices of the instance
   float* acc = reinterpret_cast<float*>(bm + a.bmat_slot);   // this CTA's block cotangents
   double* red = reinterpret_cast<double*>(acc + 2 * a.gacc_slot);
@@ -1323,32 +1409,37 @@ __global__ void __launch_bounds__(512, 1) k_batch_rs(ClusterArgs ca) {
     for (int j = lt; j < nloc; j += gs) sp[j] = make_float2((gbase | static_cast<uint32_t>(j)) == 0 ? 1.f : 0.f, 0.f);
     cluster.sync();
     const RStage* SS = ca.stg + P.stg_off;
-    const ROp* OPS = ca.rop;
+    const RPacked* OPS = ca.rop;
     const int ntb = P.n - 4;
-    // forward
+    // forward; a distributed stage needs a cluster barrier before it (unless
+    // the stage before it was distributed too) and after it
+    bool prev_dist = false;
     for (int s = 0; s < P.n_stg; ++s) {
-      const RStage* S = SS + s;
-      const bool dist = S->dist != 0;
-      const uint32_t g0 = rs_base(S, T, ntb);
-      const uint32_t r0 = 1u << S->rpos[0], r1 = 1u << S->rpos[1], r2 = 1u << S->rpos[2], r3 = 1u << S->rpos[3];
+      int dist, ob, oe;
+      const RSAddr A = rs_addr(SS + s, T, ntb, lb, dist, ob, oe);
       float2 v[16];
       if (dist) {
-        cluster.sync();
-        rs_move_dist<false>(cluster, v, sp, g0, r0, r1, r2, r3, lb);
+        if (!prev_dist) cluster.sync();
+        rs_move_dist<false>(v, sp_s, A.base, A.c0, A.s[0], A.s[1], A.s[2], A.s[3], A.k[0], A.k[1], A.k[2], A.k[3]);
       } else {
-        rs_move_local<false>(v, sp, rs_swz(g0 & lmask), rs_swz(r0), rs_swz(r1), rs_swz(r2), rs_swz(r3));
+        rs_move_local<false>(v, sp, A.base, A.s[0], A.s[1], A.s[2], A.s[3]);
       }
-      for (int o = S->op_begin; o < S->op_end; ++o) {
-        const ROp op = OPS[o];
-        rs_fwd_op(v, op, bm, g0);
+      if (ob < oe) {
+        RPacked nx = OPS[ob];
+        for (int o = ob; o < oe; ++o) {
+          const RPacked cur = nx;
+          if (o + 1 < oe) nx = OPS[o + 1];
+          rs_fwd_op(v, rs_unpack(cur), bm, A.g0);
+        }
       }
       if (dist) {
-        rs_move_dist<true>(cluster, v, sp, g0, r0, r1, r2, r3, lb);
+        rs_move_dist<true>(v, sp_s, A.base, A.c0, A.s[0], A.s[1], A.s[2], A.s[3], A.k[0], A.k[1], A.k[2], A.k[3]);
         cluster.sync();
       } else {
-        rs_move_local<true>(v, sp, rs_swz(g0 & lmask), rs_swz(r0), rs_swz(r1), rs_swz(r2), rs_swz(r3));
+        rs_move_local<true>(v, sp, A.base, A.s[0], A.s[1], A.s[2], A.s[3]);
         __syncthreads();
       }
+      prev_dist = dist != 0;
     }
     cluster.sync();
     // expectation values (partial sums per CTA, added by rank 0) and the seed of lambda
@@ -1377,35 +1468,37 @@ __global__ void __launch_bounds__(512, 1) k_batch_rs(ClusterArgs ca) {
       a.expval[I.out_off + lt] = a.obs[P.obs_off + lt].coeff * tot;
     }
     // adjoint: stages in reverse, each stage's ops in reverse
+    prev_dist = true;  // the barrier after the expectation values
     for (int s = P.n_stg - 1; s >= 0; --s) {
-      const RStage* S = SS + s;
-      const bool dist = S->dist != 0;
-      const uint32_t g0 = rs_base(S, T, ntb);
-      const uint32_t r0 = 1u << S->rpos[0], r1 = 1u << S->rpos[1], r2 = 1u << S->rpos[2], r3 = 1u << S->rpos[3];
+      int dist, ob, oe;
+      const RSAddr A = rs_addr(SS + s, T, ntb, lb, dist, ob, oe);
       float2 vp[16], vl[16];
       if (dist) {
-        cluster.sync();
-        rs_move_dist<false>(cluster, vp, sp, g0, r0, r1, r2, r3, lb);
-        rs_move_dist<false>(cluster, vl, sl, g0, r0, r1, r2, r3, lb);
+        if (!prev_dist) cluster.sync();
+        rs_move_dist<false>(vp, sp_s, A.base, A.c0, A.s[0], A.s[1], A.s[2], A.s[3], A.k[0], A.k[1], A.k[2], A.k[3]);
+        rs_move_dist<false>(vl, sl_s, A.base, A.c0, A.s[0], A.s[1], A.s[2], A.s[3], A.k[0], A.k[1], A.k[2], A.k[3]);
       } else {
-        const uint32_t base = rs_swz(g0 & lmask);
-        rs_move_local<false>(vp, sp, base, rs_swz(r0), rs_swz(r1), rs_swz(r2), rs_swz(r3));
-        rs_move_local<false>(vl, sl, base, rs_swz(r0), rs_swz(r1), rs_swz(r2), rs_swz(r3));
+        rs_move_local<false>(vp, sp, A.base, A.s[0], A.s[1], A.s[2], A.s[3]);
+        rs_move_local<false>(vl, sl, A.base, A.s[0], A.s[1], A.s[2], A.s[3]);
       }
-      for (int o = S->op_end - 1; o >= S->op_begin; --o) {
-        const ROp op = OPS[o];
-        rs_adj_op(vp, vl, op, bm, g0, acc, lane);
+      if (ob < oe) {
+        RPacked nx = OPS[oe - 1];
+        for (int o = oe - 1; o >= ob; --o) {
+          const RPacked cur = nx;
+          if (o > ob) nx = OPS[o - 1];
+          rs_adj_op(vp, vl, rs_unpack(cur), bm, A.g0, acc, lane);
+        }
       }
       if (dist) {
-        rs_move_dist<true>(cluster, vp, sp, g0, r0, r1, r2, r3, lb);
-        rs_move_dist<true>(cluster, vl, sl, g0, r0, r1, r2, r3, lb);
+        rs_move_dist<true>(vp, sp_s, A.base, A.c0, A.s[0], A.s[1], A.s[2], A.s[3], A.k[0], A.k[1], A.k[2], A.k[3]);
+        rs_move_dist<true>(vl, sl_s, A.base, A.c0, A.s[0], A.s[1], A.s[2], A.s[3], A.k[0], A.k[1], A.k[2], A.k[3]);
         cluster.sync();
       } else {
-        const uint32_t base = rs_swz(g0 & lmask);
-        rs_move_local<true>(vp, sp, base, rs_swz(r0), rs_swz(r1), rs_swz(r2), rs_swz(r3));
-        rs_move_local<true>(vl, sl, base, rs_swz(r0), rs_swz(r1), rs_swz(r2), rs_swz(r3));
+        rs_move_local<true>(vp, sp, A.base, A.s[0], A.s[1], A.s[2], A.s[3]);
+        rs_move_local<true>(vl, sl, A.base, A.s[0], A.s[1], A.s[2], A.s[3]);
         __syncthreads();
       }
+      prev_dist = dist != 0;
     }
     cluster.sync();  // every CTA's cotangent contributions are in
     for (int e = static_cast<int>(rank) * gs + lt; e < P.grad_stride; e += CL * gs) {
@@ -1465,7 +1558,7 @@ struct jq_batch {
   std::vector<double> cpool;
   std::vector<jq::DevObs> obs;
   std::vector<jq::RStage> rstg;  // register-stage programs of the cluster-class plans
-  std::vector<jq::ROp> rop;
+  std::vector<jq::RPacked> rop;
   std::vector<int> n_of_plan;   // qubit count per plan
   // configuration (autotuned)
   jq_batch_config cfg{};
@@ -1534,7 +1627,8 @@ int64_t plan_cost(const jq_batch* b, int p) {
 // rs_swz), the other lane bits the next local positions, the CTA-rank bits
 // of the thread index what is left, rank positions last (a stage without a
 // rank register bit therefore stays inside each CTA's slice).
-void build_rstages(const BBlock* bb, int nblocks, int n, int lb, std::vector<RStage>* stg, std::vector<ROp>* rops) {
+void build_rstages(const BBlock* bb, int nblocks, int n, int lb, std::vector<RStage>* stg,
+                   std::vector<RPacked>* rops) {
   std::vector<int> rem(nblocks);
   for (int i = 0; i < nblocks; ++i) rem[i] = i;
   while (!rem.empty()) {
@@ -1564,7 +1658,7 @@ void build_rstages(const BBlock* bb, int nblocks, int n, int lb, std::vector<RSt
     for (int pos = 0; pos < 32; ++pos) rix[pos] = -1;
     for (int pos = 0; pos < n; ++pos)
       if (R >> pos & 1u) {
-        st.rpos[nr] = static_cast<uint8_t>(pos);
+        st.rpos |= static_cast<uint32_t>(pos) << (8 * nr);
         rix[pos] = nr++;
       }
     std::vector<int> first, rest;
@@ -1582,7 +1676,7 @@ void build_rstages(const BBlock* bb, int nblocks, int n, int lb, std::vector<RSt
     first.insert(first.end(), rest.begin(), rest.end());
     for (int pos = lb; pos < n; ++pos)
       if (!(R >> pos & 1u)) first.push_back(pos);
-    for (size_t i = 0; i < first.size(); ++i) st.tpos[i] = static_cast<uint8_t>(first[i]);
+    for (size_t i = 0; i < first.size(); ++i) st.tpos[i / 4] |= static_cast<uint32_t>(first[i]) << (8 * (i % 4));
     st.dist = (R >> lb) != 0 ? 1 : 0;
     st.op_begin = static_cast<int32_t>(rops->size());
     for (int o : members) {
@@ -1606,7 +1700,7 @@ void build_rstages(const BBlock* bb, int nblocks, int n, int lb, std::vector<RSt
       r.perm = B.perm;
       if (B.nt == 2)
         for (int q = 0; q < 4; ++q) r.iperm |= q << (2 * ((B.perm >> (2 * q)) & 3));
-      rops->push_back(r);
+      rops->push_back(rs_pack(r));
     }
     st.op_end = static_cast<int32_t>(rops->size());
     stg->push_back(st);
@@ -1781,11 +1875,11 @@ int batch_classify(jq_batch* b, bool dry) {
   if (b->d_rop) cudaFree(b->d_rop);
   b->d_rstg = b->d_rop = nullptr;
   JQ_CUDA(cudaMalloc(&b->d_rstg, std::max<size_t>(1, b->rstg.size()) * sizeof(RStage)));
-  JQ_CUDA(cudaMalloc(&b->d_rop, std::max<size_t>(1, b->rop.size()) * sizeof(ROp)));
+  JQ_CUDA(cudaMalloc(&b->d_rop, std::max<size_t>(1, b->rop.size()) * sizeof(RPacked)));
   if (!b->rstg.empty())
     JQ_CUDA(cudaMemcpy(b->d_rstg, b->rstg.data(), b->rstg.size() * sizeof(RStage), cudaMemcpyHostToDevice));
   if (!b->rop.empty())
-    JQ_CUDA(cudaMemcpy(b->d_rop, b->rop.data(), b->rop.size() * sizeof(ROp), cudaMemcpyHostToDevice));
+    JQ_CUDA(cudaMemcpy(b->d_rop, b->rop.data(), b->rop.size() * sizeof(RPacked), cudaMemcpyHostToDevice));
   JQ_CUDA(cudaMemcpy(b->d_plans, b->bplans.data(), b->bplans.size() * sizeof(BPlan), cudaMemcpyHostToDevice));
   // workspace: counters, per-slot block matrices and cotangents, tile groups
   int64_t bs = 1, gsl = 1;
@@ -1916,7 +2010,7 @@ int batch_launch_cluster(jq_batch* b, int ci, const double* angles, const double
   ca.lbits = lbits;
   ca.xs_ws = w + b->ws_cl_xs + static_cast<size_t>(ci) * b->sm_count * 2 * (static_cast<size_t>(1) << lbits) * elem;
   ca.stg = static_cast<const RStage*>(b->d_rstg);
-  ca.rop = static_cast<const ROp*>(b->d_rop);
+  ca.rop = static_cast<const RPacked*>(b->d_rop);
   const int threads = b->cfg.cta_threads;
   size_t smem = batch_smem(lbits, 1, elem, a.bmat_slot);
   auto kern = k_batch_cluster<R, CL>;
