@@ -1028,37 +1028,50 @@ __device__ __forceinline__ void rs_d1(float2 (&v)[16], const float2* M, uint32_t
 
 // reverse one-target dense block: psi <- G^dagger psi, cotangent += lam psi^dagger,
 // lam <- G^dagger lam
-template <int Q>
+template <int Q, bool CTRL>
 __device__ __forceinline__ void rs_d1_adj(float2 (&vp)[16], float2 (&vl)[16], const float2* M, uint32_t crm, bool tp,
                                           float* dst, unsigned lane) {
-  // G^dagger = [[conj m00, conj m10], [conj m01, conj m11]]
+  // G^dagger = [[conj m00, conj m10], [conj m01, conj m11]]; three sweeps over
+  // the pairs (psi, cotangent, lambda) keep few values live at a time
   float2 ar, ai, br, bi, cr, ci, dr, di;
   rs_coef(M[0], ar, ai);
   rs_coef(M[2], br, bi);
   rs_coef(M[1], cr, ci);
   rs_coef(M[3], dr, di);
-  float g[8];
-#pragma unroll
-  for (int e = 0; e < 8; ++e) g[e] = 0.f;
 #pragma unroll
   for (int j = 0; j < 16; ++j) {
     if (j & (1 << Q)) continue;
     const int k = j | (1 << Q);
-    if (!(tp && ((static_cast<uint32_t>(j) & crm) == crm))) continue;
+    if (CTRL && !(tp && ((static_cast<uint32_t>(j) & crm) == crm))) continue;
     const float2 x = vp[j], y = vp[k];
-    const float2 p0 = rs_dotc(ar, ai, br, bi, x, y);
-    const float2 p1 = rs_dotc(cr, ci, dr, di, x, y);
+    vp[j] = rs_dotc(ar, ai, br, bi, x, y);
+    vp[k] = rs_dotc(cr, ci, dr, di, x, y);
+  }
+  if (dst) {
+    float g[8];
+#pragma unroll
+    for (int e = 0; e < 8; ++e) g[e] = 0.f;
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+      if (j & (1 << Q)) continue;
+      const int k = j | (1 << Q);
+      if (CTRL && !(tp && ((static_cast<uint32_t>(j) & crm) == crm))) continue;
+      acc_lconjp(g[0], g[1], vl[j], vp[j]);
+      acc_lconjp(g[2], g[3], vl[j], vp[k]);
+      acc_lconjp(g[4], g[5], vl[k], vp[j]);
+      acc_lconjp(g[6], g[7], vl[k], vp[k]);
+    }
+    rs_flush8(g, dst, lane);
+  }
+#pragma unroll
+  for (int j = 0; j < 16; ++j) {
+    if (j & (1 << Q)) continue;
+    const int k = j | (1 << Q);
+    if (CTRL && !(tp && ((static_cast<uint32_t>(j) & crm) == crm))) continue;
     const float2 u = vl[j], w = vl[k];
-    vp[j] = p0;
-    vp[k] = p1;
-    acc_lconjp(g[0], g[1], u, p0);
-    acc_lconjp(g[2], g[3], u, p1);
-    acc_lconjp(g[4], g[5], w, p0);
-    acc_lconjp(g[6], g[7], w, p1);
     vl[j] = rs_dotc(ar, ai, br, bi, u, w);
     vl[k] = rs_dotc(cr, ci, dr, di, u, w);
   }
-  if (dst) rs_flush8(g, dst, lane);
 }
 
 // forward two-target dense block on register bits (Q0 = matrix MSB, Q1)
@@ -1268,7 +1281,23 @@ __device__ __forceinline__ void rs_adj_op(float2 (&vp)[16], float2 (&vl)[16], co
   const uint32_t crm = op.crm;
   float* dst = op.grad_off >= 0 ? acc + 2 * op.grad_off : nullptr;
   switch (op.kind) {
-    case RO_DENSE1: JQ_RS_ONE(rs_d1_adj, vp, vl, M, crm, tp, dst, lane) break;
+    case RO_DENSE1:
+      if (crm == 0 && op.ctm == 0) {
+        switch (op.q0) {
+          case 0: rs_d1_adj<0, false>(vp, vl, M, crm, tp, dst, lane); break;
+          case 1: rs_d1_adj<1, false>(vp, vl, M, crm, tp, dst, lane); break;
+          case 2: rs_d1_adj<2, false>(vp, vl, M, crm, tp, dst, lane); break;
+          default: rs_d1_adj<3, false>(vp, vl, M, crm, tp, dst, lane); break;
+        }
+      } else {
+        switch (op.q0) {
+          case 0: rs_d1_adj<0, true>(vp, vl, M, crm, tp, dst, lane); break;
+          case 1: rs_d1_adj<1, true>(vp, vl, M, crm, tp, dst, lane); break;
+          case 2: rs_d1_adj<2, true>(vp, vl, M, crm, tp, dst, lane); break;
+          default: rs_d1_adj<3, true>(vp, vl, M, crm, tp, dst, lane); break;
+        }
+      }
+      break;
     case RO_DENSE2: JQ_RS_PAIRS(rs_d2_adj, vp, vl, M, crm, tp, dst, lane) break;
     case RO_DIAG: rs_diag_adj(vp, vl, M, op, tp, dst, lane); break;
     case RO_PERM1:
