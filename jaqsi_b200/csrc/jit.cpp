@@ -412,6 +412,16 @@ int jit_bufs() {
 
 namespace {
 
+// Consecutive register stages a then b with the warp-index thread bits
+// (above the 5 lane bits) on the same tile positions: every warp reads in b
+// exactly the amplitudes it wrote in a, so a warp barrier orders them.
+bool warp_owned(const Step& a, const Step& b, int nthb) {
+  if (a.kind != 0 || b.kind != 0 || nthb <= 5) return false;
+  for (int i = 5; i < nthb; ++i)
+    if (a.tbits[i] != b.tbits[i]) return false;
+  return true;
+}
+
 // Emit the kernel of pass p (register-stage program only).
 void emit_pass(std::ostringstream& o, const jq_plan* plan, const Schedule& s, int p, bool c64, int rb) {
   const PassDesc& pd = s.passes[p];
@@ -723,7 +733,8 @@ void emit_pass(std::ostringstream& o, const jq_plan* plan, const Schedule& s, in
       o << "    }\n";
     } else {
       for (int j = 0; j < nr; ++j) o << "      s[tb" << nstage << " ^ " << off[j] << "u] = " << outv(j) << ";\n";
-      o << "    }\n    __syncthreads();\n";
+      o << "    }\n    " << (si + 1 < pd.step_end && warp_owned(st, s.steps[si + 1], t - rb) ? "__syncwarp()" : "__syncthreads()")
+        << ";\n";
     }
     ++nstage;
   }
@@ -1025,7 +1036,9 @@ void emit_adj_pass(std::ostringstream& o, const jq_plan* plan, const Schedule& s
       for (int j = 0; j < nr; ++j)
         o << "      sp[tb" << k << " ^ " << off[j] << "u] = p" << var[j] << "; sl[tb" << k << " ^ " << off[j]
           << "u] = l" << var[j] << ";\n";
-      o << "    }\n    __syncthreads();\n";
+      o << "    }\n    "
+        << (si > pd.step_begin && warp_owned(st, s.steps[si - 1], t - rb) ? "__syncwarp()" : "__syncthreads()")
+        << ";\n";
     }
   }
   if (!direct) {
@@ -1268,7 +1281,9 @@ void emit_bwd_pass(std::ostringstream& o, const jq_plan* plan, const Schedule& s
     for (int j = 0; j < nr; ++j) o << "      " << T << " v" << j << " = src[tb" << k << " ^ " << offs[k][j] << "u];\n";
     for (int ri = st.a; ri < st.b; ++ri) emit_fwd_rop(o, s.rops[ri], c64, "v", var, nr);
     for (int j = 0; j < nr; ++j) o << "      dst[tb" << k << " ^ " << offs[k][j] << "u] = v" << var[j] << ";\n";
-    o << "    }\n    __syncthreads();\n";
+    o << "    }\n    "
+      << (k + 1 < nst && warp_owned(st, s.steps[pd.step_begin + k + 1], t - rb) ? "__syncwarp()" : "__syncthreads()")
+      << ";\n";
   }
   // reverse walk over the stages
   for (int k = nst - 1; k >= 0; --k) {
@@ -1418,7 +1433,9 @@ void emit_bwd_pass(std::ostringstream& o, const jq_plan* plan, const Schedule& s
       o << "    }\n";
     } else {
       for (int j = 0; j < nr; ++j) o << "      sl[tb" << k << " ^ " << offs[k][j] << "u] = l" << lvar[j] << ";\n";
-      o << "    }\n    __syncthreads();\n";
+      o << "    }\n    "
+        << (k > 0 && warp_owned(st, s.steps[pd.step_begin + k - 1], t - rb) ? "__syncwarp()" : "__syncthreads()")
+        << ";\n";
     }
   }
   if (!direct) o << "    " << (c64 ? "store8t" : "store16t") << tpl << "(sl, lam + goff, tbl);\n";
