@@ -63,6 +63,11 @@ TILE_PASS_TRAFFIC = {(24, "c64"): 209.3e6}
 SMEM_NOMINAL_GBS = 148 * 128 * 1.965
 
 
+def _z_reads(n_obs):
+    """Reads of the state by the Z-string measurement: one per 32 words (n >= 9)."""
+    return math.ceil(n_obs / 32)
+
+
 def _peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -625,7 +630,7 @@ def sweep_leg(args, dt_name, dev, steps, warmup, flush, max_over_ranks=lambda x:
 
         e2e_ms = max_over_ranks(_event_ms(e2e_step, steps, warmup=max(1, warmup), flush=flush))
     S = 1 << n
-    meas_reads = math.ceil(plan.n_obs / 16)
+    meas_reads = _z_reads(plan.n_obs)
     res = {
         "plan": plan, "P": P, "step_ms": step_ms, "sweep_ms": sweep_ms, "e2e_ms": e2e_ms, "expvals": ev,
         "bytes_step": (2 * P + meas_reads) * S * elem, "pass_bytes": 2 * S * elem, "meas_reads": meas_reads,
@@ -721,7 +726,7 @@ def adjoint_20q_leg(dev, steps, cpu, hbm_peak, l2_gbs):
         elem = 8 if name == "c64" else 16
         S = 1 << n
         pf, pa = plan.info["n_passes_fwd"], plan.info["n_passes_adj"]
-        bytes_ = (2 * pf + math.ceil(plan.n_obs / 16) + 2 + 4 * pa) * S * elem
+        bytes_ = (2 * pf + _z_reads(plan.n_obs) + 2 + 4 * pa) * S * elem
         achieved = bytes_ / (dev_ms * 1e-3) / 1e9
         out[name] = {
             "ms_per_grad": ms, "grads_per_s": 1e3 / ms, "device_ms_per_grad": dev_ms,

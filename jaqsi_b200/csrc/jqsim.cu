@@ -1652,6 +1652,88 @@ __global__ void __launch_bounds__(256, 2) k_expval_zdiag_sv(const typename CplxT
   if (tid < o_cnt) atomicAdd(&out[static_cast<int64_t>(inst) * n_obs + o_begin + tid], sc[tid] * acc[0]);
 }
 
+// Z strings, up to kZMax words in one read of the state (n >= 9).  A warp
+// takes 512-amplitude chunks with contiguous 16-byte loads: lane l's k-th
+// load is element 32 k + l of the chunk, so a thread's 16 amplitudes vary in
+// index bits {0, 6, 7, 8} (complex64, two amplitudes a load) or {5, 6, 7, 8}
+// (complex128).  The thread forms the 16 Walsh sums of their probabilities;
+// a word's bits on those four positions pick one sum, its parity on the
+// thread's other index bits gives the sign.  Float64 sums throughout.
+constexpr int kZMax = 32;
+
+template <typename R>
+__global__ void __launch_bounds__(256) k_expval_zstr_sv(const typename CplxT<R>::T* psi, int64_t dim,
+                                                        const DevObs* obs, int o_begin, int o_cnt, double* out,
+                                                        int n_obs) {
+  using C = typename CplxT<R>::T;
+  constexpr bool F = sizeof(C) == 8;
+  __shared__ double red[8 * kRedSlots];
+  __shared__ uint64_t sz[kZMax];
+  __shared__ int sm[kZMax];
+  __shared__ double sc[kZMax];
+  __shared__ double sw[16][256];
+  const int tid = threadIdx.x;
+  if (tid < kZMax) {
+    const bool on = tid < o_cnt;
+    const uint64_t z = on ? obs[o_begin + tid].z_mask : 0;
+    sz[tid] = z;
+    sm[tid] = F ? static_cast<int>((z & 1) | ((z >> 5) & 14)) : static_cast<int>((z >> 5) & 15);
+    sc[tid] = on ? obs[o_begin + tid].coeff : 0.0;
+  }
+  __syncthreads();
+  const int lane = tid & 31, warp = tid >> 5, nw = static_cast<int>(blockDim.x >> 5);
+  const int inst = blockIdx.y;
+  const C* p = psi + static_cast<int64_t>(inst) * dim;
+  double acc[kZMax];
+#pragma unroll
+  for (int o = 0; o < kZMax; ++o) acc[o] = 0.0;
+  const int64_t nchunk = dim >> 9;
+  for (int64_t ch = static_cast<int64_t>(blockIdx.x) * nw + warp; ch < nchunk;
+       ch += static_cast<int64_t>(gridDim.x) * nw) {
+    double w[16];
+    if constexpr (F) {
+      const float4* q = reinterpret_cast<const float4*>(p + (ch << 9));
+      float4 v[8];
+#pragma unroll
+      for (int k = 0; k < 8; ++k) v[k] = __ldcs(q + 32 * k + lane);
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        w[2 * k] = static_cast<double>(v[k].x) * v[k].x + static_cast<double>(v[k].y) * v[k].y;
+        w[2 * k + 1] = static_cast<double>(v[k].z) * v[k].z + static_cast<double>(v[k].w) * v[k].w;
+      }
+    } else {
+      const double2* q = reinterpret_cast<const double2*>(p + (ch << 9));
+      double2 v[16];
+#pragma unroll
+      for (int k = 0; k < 16; ++k) v[k] = __ldcs(q + 32 * k + lane);
+#pragma unroll
+      for (int k = 0; k < 16; ++k) w[k] = v[k].x * v[k].x + v[k].y * v[k].y;
+    }
+    // Walsh-Hadamard transform over the 4 group bits: w[m] = sum_j p_j (-1)^popc(j & m)
+#pragma unroll
+    for (int b = 1; b < 16; b <<= 1)
+#pragma unroll
+      for (int j = 0; j < 16; ++j)
+        if (!(j & b)) {
+          const double a = w[j], c = w[j | b];
+          w[j] = a + c;
+          w[j | b] = a - c;
+        }
+#pragma unroll
+    for (int m = 0; m < 16; ++m) sw[m][tid] = w[m];
+    const uint64_t gb = (static_cast<uint64_t>(ch) << 9) | static_cast<uint64_t>(F ? (lane << 1) : lane);
+#pragma unroll
+    for (int o = 0; o < kZMax; ++o) {
+      if (o < o_cnt) {
+        const double x = sw[sm[o]][tid];
+        acc[o] += (__popcll(gb & sz[o]) & 1) ? -x : x;
+      }
+    }
+  }
+  block_reduce<kZMax>(acc, red);
+  if (tid < o_cnt) atomicAdd(&out[static_cast<int64_t>(inst) * n_obs + o_begin + tid], sc[tid] * acc[0]);
+}
+
 // General Pauli words: <psi| coeff P |psi> = coeff sum_j conj(psi_j) phase(j ^ x) psi_{j ^ x}.
 template <typename R>
 __global__ void __launch_bounds__(256, 2) k_expval_pauli_sv(const typename CplxT<R>::T* psi, int64_t dim,
@@ -2220,10 +2302,13 @@ int measure(const jq_plan* plan, const DeviceTables* T, int batch, int out_type,
     int i = 0;
     while (i < n_obs) {
       if (plan->obs[i].kind == JQ_OBS_PAULI) {
-        // runs of Pauli words that are all Z strings (or all not), kObsChunk at most
+        // runs of Pauli words that are all Z strings (or all not), kObsChunk at
+        // most (kZMax for the one-read Z-string kernel, statevectors of n >= 9)
         const bool zdiag = plan->obs[i].x_mask == 0 && (plan->obs[i].z_mask >> 35) == 0;
+        const bool zstr = zdiag && !dm && n >= 9;
+        const int chunk = zstr ? kZMax : kObsChunk;
         int j = i;
-        while (j < n_obs && j - i < kObsChunk && plan->obs[j].kind == JQ_OBS_PAULI &&
+        while (j < n_obs && j - i < chunk && plan->obs[j].kind == JQ_OBS_PAULI &&
                (plan->obs[j].x_mask == 0 && (plan->obs[j].z_mask >> 35) == 0) == zdiag)
           ++j;
         const int gx = std::max(1, std::min<int>(static_cast<int>((dim + threads - 1) / threads),
@@ -2234,7 +2319,12 @@ int measure(const jq_plan* plan, const DeviceTables* T, int batch, int out_type,
           const C* sb = state + static_cast<int64_t>(b0) * plan->state_elems;
           double* ob = o + static_cast<int64_t>(b0) * n_obs;
           if (dm) k_expval_pauli_dm<R><<<grid, threads, 0, st>>>(sb, dim, od, i, j - i, ob, n_obs);
-          else if (zdiag) k_expval_zdiag_sv<R><<<grid, threads, 0, st>>>(sb, dim, od, i, j - i, ob, n_obs);
+          else if (zstr) {
+            // one warp per 512-amplitude chunk
+            const int gz = std::max(1, std::min<int>(static_cast<int>((dim >> 9) / (threads / 32)) + 1,
+                                                     std::max(1, 4 * sm_count() / std::max(batch, 1))));
+            k_expval_zstr_sv<R><<<dim3(gz, grid.y), threads, 0, st>>>(sb, dim, od, i, j - i, ob, n_obs);
+          } else if (zdiag) k_expval_zdiag_sv<R><<<grid, threads, 0, st>>>(sb, dim, od, i, j - i, ob, n_obs);
           else k_expval_pauli_sv<R><<<grid, threads, 0, st>>>(sb, dim, od, i, j - i, ob, n_obs);
         }
         i = j;

@@ -517,3 +517,31 @@ def test_batch_beyond_grid_y_limit():
     want = torch.zeros_like(counts)
     want[torch.arange(batch), torch.arange(batch) % dim] = shots
     assert torch.equal(counts, want)
+
+
+@pytest.mark.parametrize("dtype", DTYPES)
+@pytest.mark.parametrize("n", [9, 12])
+def test_many_z_strings_one_read(n, dtype):
+    """Z-string observables on n >= 9 qubits read the state once per 32 words
+    (Walsh sums over 16 amplitudes a thread): 40 random words of weight 1..n,
+    three batched parameter sets, against the oracle."""
+    rng = np.random.default_rng(70 + n)
+    words = []
+    for _ in range(40):
+        k = int(rng.integers(1, n + 1))
+        words.append(sorted(int(w) for w in rng.choice(n, k, replace=False)))
+    obs = [jq.PauliZ(wires=w[0]) if len(w) == 1 else jq.build_parity_observable(w) for w in words]
+    npar = count_params(n, 60, n)
+    params = torch.tensor(np.random.default_rng(7).uniform(0, 2 * np.pi, (3, npar + 1)))
+
+    def circuit(p):
+        for w in range(n):
+            jq.H(wires=w)
+        random_circuit(n, 60, np.random.default_rng(n), p)
+
+    script = jq.Script(circuit, n_qubits=n)
+    got = _np(script.execute("expval", obs, args=(params,), in_axes=(0,), dtype=dtype))
+    for b in range(3):
+        recs = to_records(script.record(params[b]))
+        want = O.expval_state(O.simulate_pure(recs, n), n, obs_records(obs))
+        np.testing.assert_allclose(got[b], want, atol=TOL[dtype])
