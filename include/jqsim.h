@@ -136,6 +136,19 @@ typedef struct jq_tune {
                             interpreter runs), 1 on (a failed specialisation
                             fails every call on that device with its error
                             text), -1 off (register-stage interpreter only)    */
+  int32_t expval_only;   /* nonzero: the plan is run for expectation values
+                            only (jq_forward / jq_adjoint / jq_backward with
+                            JQ_OUT_EXPVAL).  When every observable is a Z
+                            string (Pauli, no X or Y) of a statevector plan,
+                            trailing blocks that are affine permutations of
+                            the index bits (X, CX, SWAP and their fusions) or
+                            constant diagonal unitaries are absorbed into the
+                            words (P psi with P(i) = A i ^ b gives
+                            <Z_z> = (-1)^popc(z & b) <Z_{A^T z}> before P)
+                            and not run; the state buffers then hold the
+                            state before them (jq_sweep applies the passes
+                            the plan keeps), and other out types fail with
+                            JQ_EINVAL.                                         */
 } jq_tune;
 
 /* Plan summary. */

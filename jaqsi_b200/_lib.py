@@ -109,6 +109,7 @@ class JqTune(ctypes.Structure):
         ("no_fuse", ctypes.c_int32),
         ("ckpt_stride", ctypes.c_int32),
         ("jit", ctypes.c_int32),
+        ("expval_only", ctypes.c_int32),
     ]
 
 

@@ -192,5 +192,6 @@ struct jq_plan {
   int ckpt_stride = 0;
   bool jit = false;             // specialise the forward passes with NVRTC
   bool jit_required = false;    // jq_tune.jit = 1: a failed specialisation is an error
+  int absorbed = 0;             // trailing blocks absorbed into the Z strings (jq_tune.expval_only)
   std::deque<jq::DeviceTables> dev;  // per-device uploads (a deque: references stay valid as devices are added)
 };

@@ -2856,6 +2856,18 @@ size_t jq_workspace_bytes(const jq_plan* plan, int batch, int out_type, int with
   return layout(plan, batch, mode).total;
 }
 
+// A plan that absorbed trailing blocks into its Z strings (jq_tune.expval_only)
+// is run for expectation values only.
+static int check_expval_only(const jq_plan* plan, int out_type, const char* who) {
+  if (plan->absorbed > 0 && out_type != JQ_OUT_EXPVAL) {
+    set_error(std::string(who) + ": the plan was built with jq_tune.expval_only and absorbed " +
+              std::to_string(plan->absorbed) + " trailing blocks into its observables; it measures "
+              "expectation values only");
+    return JQ_EINVAL;
+  }
+  return JQ_OK;
+}
+
 static int check_common(const jq_plan* plan, int batch, const double* angles, const void* mats) {
   if (!plan) { set_error("NULL plan"); return JQ_EINVAL; }
   if (batch < 1) { set_error("batch must be >= 1"); return JQ_EINVAL; }
@@ -2869,6 +2881,7 @@ int jq_forward(const jq_plan* plan, int batch, const double* angles, const void*
                void* stream) {
   int rc = check_common(plan, batch, angles, mats);
   if (rc) return rc;
+  if ((rc = check_expval_only(plan, out_type, "jq_forward"))) return rc;
   if (!state) { set_error("jq_forward: state buffer is NULL"); return JQ_EINVAL; }
   if (out_type != JQ_OUT_STATE && !(out_type == JQ_OUT_DENSITY && plan->mode == JQ_DENSITY) && !out &&
       !(out_type == JQ_OUT_EXPVAL && plan->obs.empty())) {
@@ -2898,6 +2911,7 @@ int jq_adjoint(const jq_plan* plan, int batch, const double* angles, const void*
                void* grad_init, void* workspace, size_t workspace_bytes, void* stream) {
   int rc = check_common(plan, batch, angles, mats);
   if (rc) return rc;
+  if ((rc = check_expval_only(plan, out_type, "jq_adjoint"))) return rc;
   if (!state) { set_error("jq_adjoint: state is NULL"); return JQ_EINVAL; }
   if (out_type == JQ_OUT_EXPVAL ? (!ct && !plan->obs.empty()) : !ct_state) {
     set_error("jq_adjoint: missing cotangent");
@@ -2916,6 +2930,7 @@ int jq_backward(const jq_plan* plan, int batch, const double* angles, const void
                 void* grad_mats, void* grad_init, void* workspace, size_t workspace_bytes, void* stream) {
   int rc = check_common(plan, batch, angles, mats);
   if (rc) return rc;
+  if ((rc = check_expval_only(plan, out_type, "jq_backward"))) return rc;
   if (out_type == JQ_OUT_EXPVAL ? (!ct && !plan->obs.empty()) : !ct_state) {
     set_error("jq_backward: missing cotangent");
     return JQ_EINVAL;
@@ -2946,6 +2961,7 @@ int jq_forward_noalloc(const jq_plan* plan, int batch, const double* angles, con
                        int init_batched, int out_type, void* state, void* out, void* stream) {
   int rc = check_common(plan, batch, angles, mats);
   if (rc) return rc;
+  if ((rc = check_expval_only(plan, out_type, "jq_forward_noalloc"))) return rc;
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) {
     set_error("jq_forward_noalloc: no current CUDA device");

@@ -617,6 +617,69 @@ int build_plan(const jq_op* ops, int n_ops, const jq_obs* obs, int n_obs, int n_
     }
   }
 
+  // ---- trailing blocks absorbed into Z-string observables -------------------
+  // (jq_tune.expval_only, statevector, every observable a Z string).  From the
+  // end of the circuit: a constant diagonal unitary commutes with every Z
+  // string and is dropped; a constant permutation that is affine over the
+  // index bits, P(i) = A i ^ b, is dropped after each word z becomes A^T z
+  // with the sign (-1)^popc(z & b).  Blocks with parameters stop the walk.
+  std::vector<uint64_t> zt;
+  std::vector<double> zsign;
+  if (tune && tune->expval_only && mode == JQ_STATEVECTOR && n_obs > 0) {
+    bool all_z = true;
+    for (int i = 0; i < n_obs; ++i)
+      if (obs[i].kind != JQ_OBS_PAULI || obs[i].x_mask != 0) all_z = false;
+    if (all_z) {
+      zt.resize(n_obs);
+      zsign.assign(n_obs, 1.0);
+      for (int i = 0; i < n_obs; ++i) zt[i] = obs[i].z_mask;
+      while (!blocks.empty()) {
+        const HostBlock& hb = blocks.back();
+        const int k = static_cast<int>(hb.wires.size()), dim = 1 << k;
+        bool constant = hb.unitary;
+        for (int pi : hb.prims) {
+          const int op = prims[pi].op;
+          if (op >= 0 && (plan->ops[op].n_angles > 0 || plan->ops[op].kind == JQ_K_MATRIX ||
+                          plan->ops[op].kind == JQ_K_CHANNEL))
+            constant = false;
+        }
+        if (!constant) break;
+        if (!hb.st.diagonal) {
+          if (static_cast<int>(hb.st.perm.size()) != dim) break;
+          // P(i): the row that takes input row i (out[r] = in[perm[r]])
+          std::vector<int> inv(dim);
+          for (int r = 0; r < dim; ++r) inv[hb.st.perm[r]] = r;
+          const int b0 = inv[0];
+          std::vector<int> col(k);
+          for (int m = 0; m < k; ++m) col[m] = inv[1 << m] ^ b0;
+          bool affine = true;
+          for (int x = 0; x < dim && affine; ++x) {
+            int v = b0;
+            for (int m = 0; m < k; ++m)
+              if (x >> m & 1) v ^= col[m];
+            affine = v == inv[x];
+          }
+          if (!affine) break;
+          // local bit m is wire wires[k - 1 - m], flat bit nb - 1 - that wire
+          auto gbit = [&](int m) { return nb - 1 - hb.wires[k - 1 - m]; };
+          for (int i = 0; i < n_obs; ++i) {
+            uint32_t zl = 0;
+            for (int m = 0; m < k; ++m) zl |= static_cast<uint32_t>((zt[i] >> gbit(m)) & 1ULL) << m;
+            if (__builtin_popcount(zl & static_cast<uint32_t>(b0)) & 1) zsign[i] = -zsign[i];
+            uint64_t z = zt[i];
+            for (int m = 0; m < k; ++m) {
+              const uint64_t bit = 1ULL << gbit(m);
+              z = (__builtin_popcount(zl & static_cast<uint32_t>(col[m])) & 1) ? (z | bit) : (z & ~bit);
+            }
+            zt[i] = z;
+          }
+        }
+        blocks.pop_back();
+        ++plan->absorbed;
+      }
+    }
+  }
+
   // ---- device prims / blocks -----------------------------------------------
   int maxk = 1;
   for (const HostBlock& b : blocks) maxk = std::max(maxk, static_cast<int>(b.wires.size()));
@@ -697,7 +760,10 @@ int build_plan(const jq_op* ops, int n_ops, const jq_obs* obs, int n_obs, int n_
   plan->scratch_stride = scratch;
 
   // ---- schedules ---------------------------------------------------------------
-  const int c_seed = std::min(nb, dtype == JQ_C64 ? 4 : 3);
+  // low index bits every tile holds (contiguous runs of 2^c amplitudes:
+  // 128 bytes complex64, 128 bytes complex128); JQ_TILE_LOW overrides
+  int c_seed = std::min(nb, dtype == JQ_C64 ? 4 : 3);
+  if (const char* e = std::getenv("JQ_TILE_LOW")) c_seed = std::min(nb, std::max(2, std::min(6, std::atoi(e))));
   int tf = (tune && tune->tile_bits > 0) ? tune->tile_bits : default_tile_bits(nb, dtype, maxk, c_seed, false);
   int ta = (tune && tune->tile_bits_adj > 0) ? tune->tile_bits_adj : default_tile_bits(nb, dtype, maxk, c_seed, true);
   tf = std::min(std::min(tf, nb), kMaxTileBits);
@@ -735,9 +801,9 @@ int build_plan(const jq_op* ops, int n_ops, const jq_obs* obs, int n_obs, int n_
       uint64_t lim = (n >= 64) ? ~0ULL : ((1ULL << n) - 1);
       if ((o.x_mask | o.z_mask) & ~lim) return fail("observable " + std::to_string(i) + ": Pauli mask outside the register");
       d.x_mask = o.x_mask;
-      d.z_mask = o.z_mask;
+      d.z_mask = zt.empty() ? o.z_mask : zt[i];
       d.n_y = o.n_y;
-      d.coeff = o.coeff;
+      d.coeff = zt.empty() ? o.coeff : o.coeff * zsign[i];
     } else if (o.kind == JQ_OBS_DENSE) {
       int k = o.n_wires;
       if (k < 1 || k > JQ_MAX_OP_WIRES || !o.mat) return fail("observable " + std::to_string(i) + ": bad dense observable");

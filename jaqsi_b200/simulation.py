@@ -416,6 +416,13 @@ PLAN_CACHE_SIZE = 256
 
 def get_plan(lw: Lowered, obs_specs, obs_key, n_qubits: int, mode: int, dtype: torch.dtype,
              tune: Optional[dict] = None) -> Plan:
+    """The plan of a lowered tape, memoised.  Observables are lowered only for
+    expectation values, so a statevector plan with observables is built with
+    ``expval_only``: trailing permutations and constant diagonals are then
+    absorbed into Z-string observables (the state it leaves is the one before
+    them; jaqsi measures the same values after them, simulation.py:777-801)."""
+    if obs_specs and mode == L.JQ_STATEVECTOR and not (tune or {}).get("no_fuse"):
+        tune = dict(tune or {}, expval_only=1)
     key = (lw.key, obs_key, n_qubits, mode, dtype, tuple(sorted((tune or {}).items())))
     with _PLAN_LOCK:
         plan = _PLAN_CACHE.get(key)

@@ -545,3 +545,65 @@ def test_many_z_strings_one_read(n, dtype):
         recs = to_records(script.record(params[b]))
         want = O.expval_state(O.simulate_pure(recs, n), n, obs_records(obs))
         np.testing.assert_allclose(got[b], want, atol=TOL[dtype])
+
+
+@pytest.mark.parametrize("dtype", DTYPES)
+@pytest.mark.parametrize("n,tail", [(5, "affine"), (10, "affine"), (6, "toffoli")])
+def test_trailing_permutations_absorbed_into_z_strings(n, tail, dtype):
+    """Expectation-value plans absorb trailing X / CX / SWAP / constant
+    diagonal blocks into their Z strings (jq_tune.expval_only): values and
+    angle gradients against the oracle, which runs every gate.  A Toffoli
+    (not affine) stops the absorption."""
+    rng = np.random.default_rng(90 + n)
+    npar = 3 * n
+    base = rng.uniform(0, 2 * np.pi, npar)
+
+    def circuit(p):
+        for w in range(n):
+            jq.Rot(p[3 * w], p[3 * w + 1], p[3 * w + 2], wires=w)
+        for w in range(n):
+            jq.CX(wires=[w, (w + 1) % n])
+        if tail == "toffoli":
+            jq.CCX(wires=[0, 1, 2])
+        jq.PauliX(wires=1)
+        jq.SWAP(wires=[0, n - 1])
+        jq.CZ(wires=[1, 2])
+        jq.S(wires=3)
+        jq.CX(wires=[2, 4])
+
+    obs = [jq.PauliZ(0), jq.build_parity_observable([1, 3]), jq.build_parity_observable(list(range(n))),
+           jq.PauliZ(n - 1)]
+    ct = rng.normal(size=len(obs))
+    script = jq.Script(circuit, n_qubits=n)
+    params = torch.tensor(base, requires_grad=True)
+    ev = script.execute("expval", obs, args=(params,), dtype=dtype)
+    (ev.to(torch.float64) @ torch.tensor(ct, device=ev.device)).backward()
+    recs = to_records(script.record(torch.tensor(base)))
+    ev_ref, g_ref = O.adjoint_grad(recs, n, obs_records(obs), ct=ct)
+    np.testing.assert_allclose(_np(ev), ev_ref, atol=TOL[dtype])
+    np.testing.assert_allclose(_np(params.grad), g_ref[:npar], atol=TOL[dtype] * max(1.0, np.abs(ct).sum()))
+    # the same tape's state output runs every gate
+    np.testing.assert_allclose(_np(script.execute("state", args=(params.detach(),), dtype=dtype)),
+                               O.simulate_pure(recs, n), atol=TOL[dtype])
+
+
+def test_absorbed_plan_measures_expectation_values_only():
+    from jaqsi_b200 import _lib as L
+
+    n = 4
+
+    def circuit(p):
+        jq.RY(p[0], wires=0)
+        jq.CX(wires=[0, 1])
+        jq.SWAP(wires=[1, 3])
+
+    script = jq.Script(circuit, n_qubits=n)
+    x = torch.tensor([0.4])
+    lw = sim.lower_tape(script.record(x), n)
+    specs, okey = sim._lower_obs([jq.PauliZ(3)], n)
+    plan = sim.get_plan(lw, specs, okey, n, L.JQ_STATEVECTOR, torch.complex128)
+    assert plan.info["n_blocks"] == 1  # CX and SWAP absorbed into the word
+    ev = sim.run_plan(plan, L.JQ_OUT_EXPVAL, 1, sim.gather_angles(lw.angles, torch.device("cuda")), None, None, 0)
+    np.testing.assert_allclose(_np(ev).ravel(), [np.cos(0.4)], atol=1e-12)
+    with pytest.raises(ValueError, match="expectation values only"):
+        sim.run_plan(plan, L.JQ_OUT_STATE, 1, sim.gather_angles(lw.angles, torch.device("cuda")), None, None, 0)
