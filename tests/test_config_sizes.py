@@ -122,3 +122,49 @@ def test_noisy_dm_12q_gradient_vs_central_differences():
         err = np.abs(g - fd).max()
         print(f"12q noisy density gradient {dtype}: max |reverse pass - central difference| = {err:.3e}")
         assert err <= GRAD_TOL[dtype]
+
+
+@pytest.mark.parametrize("dtype", [torch.complex64, torch.complex128])
+def test_30_qubits_largest_statevector(dtype):
+    """The largest statevector (30 qubits: 8 GiB complex64, 16 GiB
+    complex128; offsets past 2^32 bytes): a product state of RY then RZ on
+    every wire, where <Z_i> = cos(a_i) and <Z_i Z_j> = cos(a_i) cos(a_j)
+    exactly, and the gradient of sum_i <Z_i> is -sin(a_i); plus the state's
+    norm through the probabilities of a CX chain appended (a permutation)."""
+    n = 30
+    free, total = torch.cuda.mem_get_info()
+    need = (2 ** n) * (8 if dtype == torch.complex64 else 16) * 3
+    if free < need:
+        pytest.skip(f"needs {need / 2**30:.0f} GiB free on the device")
+    rng = np.random.default_rng(30)
+    a = rng.uniform(0, np.pi, n)
+    b = rng.uniform(0, 2 * np.pi, n)
+
+    def circuit(x, z):
+        for w in range(n):
+            jq.RY(x[w], wires=w)
+            jq.RZ(z[w], wires=w)
+
+    script = jq.Script(circuit, n_qubits=n)
+    x = torch.tensor(a, requires_grad=True)
+    pairs = [(0, 29), (3, 17), (28, 29), (0, 1)]
+    obs = [jq.PauliZ(w) for w in range(n)] + [jq.build_parity_observable(list(p)) for p in pairs]
+    ev = script.execute("expval", obs, args=(x, torch.tensor(b)), dtype=dtype)
+    tol = 1e-5 if dtype == torch.complex64 else 1e-10
+    want = np.concatenate([np.cos(a), [np.cos(a[i]) * np.cos(a[j]) for i, j in pairs]])
+    np.testing.assert_allclose(ev.detach().cpu().numpy(), want, atol=tol)
+    ev[:n].sum().backward()
+    np.testing.assert_allclose(x.grad.numpy(), -np.sin(a), atol=tol * 10)
+    del ev
+    torch.cuda.empty_cache()
+
+    def chained(x, z):
+        circuit(x, z)
+        for w in range(n - 1):
+            jq.CX(wires=[w, w + 1])
+
+    p = jq.Script(chained, n_qubits=n).execute("probs", args=(torch.tensor(a), torch.tensor(b)), dtype=dtype)
+    s = float(p.double().sum())
+    assert abs(s - 1.0) < (1e-4 if dtype == torch.complex64 else 1e-10), s
+    del p
+    torch.cuda.empty_cache()
