@@ -394,16 +394,22 @@ void build_steps(Schedule& s, const std::vector<int32_t>& perm_pool, int dtype) 
   }
 }
 
-int default_tile_bits(int nb, int dtype, int maxk, int c_seed, bool adjoint) {
-  // 64 KB tiles: two CTAs share an SM, so one streams its tile while the
-  // other computes (a 128 KB tile leaves the SM idle during its own copies)
+int default_tile_bits(int nb, int dtype, int maxk, int c_seed, bool adjoint, bool density, bool grad) {
   // 16 amplitudes per thread, 128 threads per tile: small tiles leave
   // several CTAs per SM to hide shared-memory and barrier latency
   int t = 11;
   if (adjoint) t = 11;
+  // Density matrices: the checkpointed reverse step keeps one tile per
+  // register stage in shared memory, so smaller tiles fit more CTAs an SM.
+  // Measured on the 12-qubit noisy circuit (forward + gradient per set):
+  // complex64 51.7 / 48.3 / 63.9 ms at 11 / 10 / 9 bits (forward alone also
+  // fastest at 10), complex128 98.4 / 93.4 / 89.2 ms (forward 13.7 / 14.1 /
+  // 14.9 ms).
+  if (density) t = (dtype == JQ_C128 && grad) ? 9 : 10;
   // keep at least ~256 tiles per state when the state is large enough
-  int floor_t = std::max(10, maxk + c_seed);
+  int floor_t = std::max(std::min(t, 10), maxk + c_seed);
   if (nb - 8 < t) t = std::max(nb - 8, floor_t);
+  t = std::max(t, maxk + c_seed);
   if (t > nb) t = nb;
   return t;
 }
@@ -764,8 +770,11 @@ int build_plan(const jq_op* ops, int n_ops, const jq_obs* obs, int n_obs, int n_
   // 128 bytes complex64, 128 bytes complex128); JQ_TILE_LOW overrides
   int c_seed = std::min(nb, dtype == JQ_C64 ? 4 : 3);
   if (const char* e = std::getenv("JQ_TILE_LOW")) c_seed = std::min(nb, std::max(2, std::min(6, std::atoi(e))));
-  int tf = (tune && tune->tile_bits > 0) ? tune->tile_bits : default_tile_bits(nb, dtype, maxk, c_seed, false);
-  int ta = (tune && tune->tile_bits_adj > 0) ? tune->tile_bits_adj : default_tile_bits(nb, dtype, maxk, c_seed, true);
+  const bool dens = mode == JQ_DENSITY;
+  int tf = (tune && tune->tile_bits > 0) ? tune->tile_bits
+                                         : default_tile_bits(nb, dtype, maxk, c_seed, false, dens, plan->any_grad);
+  int ta = (tune && tune->tile_bits_adj > 0) ? tune->tile_bits_adj
+                                             : default_tile_bits(nb, dtype, maxk, c_seed, true, dens, plan->any_grad);
   tf = std::min(std::min(tf, nb), kMaxTileBits);
   ta = std::min(std::min(ta, nb), kMaxTileBits);
   if (tf < std::min(nb, maxk + c_seed) || ta < std::min(nb, maxk + c_seed)) {
