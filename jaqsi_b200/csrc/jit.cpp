@@ -54,6 +54,7 @@ struct Driver {
                      void**, void**);
   CUresult (*set_attr)(CUfunction, CUfunction_attribute, int);
   CUresult (*occupancy)(int*, CUfunction, int, size_t);
+  CUresult (*launch_ex)(const CUlaunchConfig*, CUfunction, void**, void**) = nullptr;  // optional
 };
 
 std::once_flag g_once;
@@ -91,7 +92,50 @@ void init_bindings() {
              entry("cuModuleGetFunction", &g_drv.get_function) && entry("cuLaunchKernel", &g_drv.launch) &&
              entry("cuFuncSetAttribute", &g_drv.set_attr) &&
              entry("cuOccupancyMaxActiveBlocksPerMultiprocessor", &g_drv.occupancy);
+  if (!entry("cuLaunchKernelEx", &g_drv.launch_ex)) g_drv.launch_ex = nullptr;
 }
+
+// Generated passes start with griddepcontrol.launch_dependents and wait
+// (griddepcontrol.wait) for the preceding kernel of the stream before their
+// first global access, so back-to-back passes launched with programmatic
+// stream serialisation overlap the next pass's launch and prologue with the
+// previous pass's last tiles; the wait returns at once for a plain launch.
+// JQ_PDL is a bit mask of the pass kinds launched that way: 1 forward,
+// 2 adjoint, 4 checkpointed reverse (default 1).
+enum { kPdlFwd = 1, kPdlAdj = 2, kPdlBwd = 4 };
+int pdl_mask() {
+  static const int m = [] {
+    const char* e = std::getenv("JQ_PDL");
+    return e ? std::atoi(e) : int(kPdlFwd);
+  }();
+  return m;
+}
+
+CUresult launch_pass(CUfunction f, unsigned grid, unsigned threads, unsigned smem, cudaStream_t st, void** args,
+                     int kind) {
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  if (g_drv.launch_ex && (pdl_mask() & kind) && cudaStreamIsCapturing(st, &cap) == cudaSuccess &&
+      cap == cudaStreamCaptureStatusNone) {
+    CUlaunchAttribute attr[1];
+    std::memset(attr, 0, sizeof(attr));
+    attr[0].id = CU_LAUNCH_ATTRIBUTE_PROGRAMMATIC_STREAM_SERIALIZATION;
+    attr[0].value.programmaticStreamSerializationAllowed = 1;
+    CUlaunchConfig cfg;
+    std::memset(&cfg, 0, sizeof(cfg));
+    cfg.gridDimX = grid;
+    cfg.gridDimY = cfg.gridDimZ = 1;
+    cfg.blockDimX = threads;
+    cfg.blockDimY = cfg.blockDimZ = 1;
+    cfg.sharedMemBytes = smem;
+    cfg.hStream = reinterpret_cast<CUstream>(st);
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return g_drv.launch_ex(&cfg, f, args, nullptr);
+  }
+  return g_drv.launch(f, grid, 1, 1, threads, 1, 1, smem, reinterpret_cast<CUstream>(st), args, nullptr);
+}
+const char* kPdlTrigger = "  asm volatile(\"griddepcontrol.launch_dependents;\");\n";
+const char* kPdlWait = "  asm volatile(\"griddepcontrol.wait;\" ::: \"memory\");\n";
 
 // ---- device prelude shared by every generated kernel --------------------------
 const char* kPrelude = R"JQ(
@@ -461,6 +505,7 @@ void emit_pass(std::ostringstream& o, const jq_plan* plan, const Schedule& s, in
     o << "  u32* tbl = (u32*)(smat + " << smat_pad << ");\n";
   }
   o << "  const u32 tid = threadIdx.x;\n";
+  o << kPdlTrigger;
   // bit-deposit table of the tile's high bits
   o << "  { const u32 hb[] = {";
   for (int i = c; i < t; ++i) o << (i > c ? ", " : "") << (1u << pd.bits[i]);
@@ -514,6 +559,7 @@ void emit_pass(std::ostringstream& o, const jq_plan* plan, const Schedule& s, in
   o << "  auto gaddr = [&](long long tl) { const u64 ti = (u64)tl & (u64)(tiles_per - 1); return state + ((tl >> "
     << (nb - t) << ") << " << nb << ") + " << pdep_expr("ti", outer) << "; };\n";
   o << "  __syncthreads();\n";
+  o << kPdlWait;  // the state is read (and written) only after the previous pass completed
   for (int j = 0; j + 1 < nbuf; ++j) {
     o << "  if ((long long)blockIdx.x + " << j << "ll * gridDim.x < ntiles) " << pf << "(s0 + " << j * (1 << t)
       << ", gaddr(blockIdx.x + " << j << "ll * gridDim.x), tbl);\n";
@@ -788,6 +834,7 @@ void emit_adj_pass(std::ostringstream& o, const jq_plan* plan, const Schedule& s
   }
   o << "  u32* tbl = (u32*)(sacc + " << nacc_pad << ");\n";
   o << "  const u32 tid = threadIdx.x;\n";
+  o << kPdlTrigger << kPdlWait;
   o << "  { const u32 hb[] = {";
   for (int i = c; i < t; ++i) o << (i > c ? ", " : "") << (1u << pd.bits[i]);
   if (t == c) o << "0u";
@@ -1199,6 +1246,7 @@ void emit_bwd_pass(std::ostringstream& o, const jq_plan* plan, const Schedule& s
   }
   o << "  u32* tbl = (u32*)(sacc + " << nacc_pad << ");\n";
   o << "  const u32 tid = threadIdx.x;\n";
+  o << kPdlTrigger << kPdlWait;
   o << "  { const u32 hb[] = {";
   for (int i = c; i < t; ++i) o << (i > c ? ", " : "") << (1u << pd.bits[i]);
   if (t == c) o << "0u";
@@ -1689,8 +1737,8 @@ int jit_launch(const JitModule& m, const Schedule& s, int p, int n_bits, int sm_
   long long bs = bstride;
   const int32_t* mc = static_cast<const int32_t*>(m.mc) + m.mc_off[p];
   void* args[] = {&state, &batch, const_cast<void**>(&bmat), &bs, &mc, &out};
-  if (g_drv.launch(f, grid, 1, 1, threads, 1, 1, static_cast<unsigned>(smem), reinterpret_cast<CUstream>(st), args,
-                   nullptr) != CUDA_SUCCESS) {
+  if (launch_pass(f, grid, static_cast<unsigned>(threads), static_cast<unsigned>(smem), st, args, kPdlFwd) !=
+      CUDA_SUCCESS) {
     set_error("cuLaunchKernel failed for a specialised pass");
     return JQ_ECUDA;
   }
@@ -1728,8 +1776,8 @@ int jit_launch_adj(const JitModule& m, const Schedule& s, int p, int n_bits, int
   const int32_t* mc = static_cast<const int32_t*>(m.mc) + m.mc_off[p];
   const int32_t* gt = static_cast<const int32_t*>(m.gt) + m.gt_off[p];
   void* args[] = {&psi, &lam, &batch, const_cast<void**>(&bmat), &bs, &mc, &gacc, &gs, &gt};
-  if (g_drv.launch(f, grid, 1, 1, threads, 1, 1, static_cast<unsigned>(smem), reinterpret_cast<CUstream>(st), args,
-                   nullptr) != CUDA_SUCCESS) {
+  if (launch_pass(f, grid, static_cast<unsigned>(threads), static_cast<unsigned>(smem), st, args, kPdlAdj) !=
+      CUDA_SUCCESS) {
     set_error("cuLaunchKernel failed for a specialised adjoint pass");
     return JQ_ECUDA;
   }
@@ -1754,8 +1802,8 @@ int jit_launch_bwd(const JitModule& m, const Schedule& s, int p, int n_bits, int
   const int32_t* gt = static_cast<const int32_t*>(m.gt) + m.gt_off[p];
   void* xp = const_cast<void*>(xin);
   void* args[] = {&xp, &lam, &batch, const_cast<void**>(&bmat), &bs, &mc, &gacc, &gs, &gt};
-  if (g_drv.launch(f, grid, 1, 1, threads, 1, 1, static_cast<unsigned>(smem), reinterpret_cast<CUstream>(st), args,
-                   nullptr) != CUDA_SUCCESS) {
+  if (launch_pass(f, grid, static_cast<unsigned>(threads), static_cast<unsigned>(smem), st, args, kPdlBwd) !=
+      CUDA_SUCCESS) {
     set_error("cuLaunchKernel failed for a specialised reverse pass");
     return JQ_ECUDA;
   }
