@@ -454,6 +454,17 @@ int jit_bufs() {
   return n;
 }
 
+// Tile order of consecutive forward passes: alternately ascending and
+// descending, so that each pass starts on the tiles the pass before it wrote
+// last (24-qubit sweep: -1% a step); JQ_JIT_REV=0 keeps every pass ascending.
+bool alternate_tile_order() {
+  static const bool on = [] {
+    const char* e = std::getenv("JQ_JIT_REV");
+    return !(e && std::atoi(e) == 0);
+  }();
+  return on;
+}
+
 namespace {
 
 // Consecutive register stages a then b with the warp-index thread bits
@@ -490,7 +501,7 @@ void emit_pass(std::ostringstream& o, const jq_plan* plan, const Schedule& s, in
   // in-place pass, another one for the checkpointed reverse pass's recompute)
   o << "extern \"C\" __global__ void __launch_bounds__(" << nthr << ", " << minb << ") @KERNEL@(" << T
     << "* state, int batch, const " << T << "* __restrict__ bmat, long long bstride, "
-    << "const int* __restrict__ mc, " << T << "* out) {\n";
+    << "const int* __restrict__ mc, " << T << "* out, int rev) {\n";
   // nbuf tile buffers: the next nbuf - 1 tiles stream in (cp.async) while
   // this one is computed
   const int nbuf = jit_bufs();
@@ -556,7 +567,11 @@ void emit_pass(std::ostringstream& o, const jq_plan* plan, const Schedule& s, in
   const std::string pf = (c64 ? "prefetch8t" : "prefetch16t") + tpl;
   o << "  const long long tiles_per = 1ll << " << (nb - t) << ";\n";
   o << "  const long long ntiles = tiles_per * batch;\n";
-  o << "  auto gaddr = [&](long long tl) { const u64 ti = (u64)tl & (u64)(tiles_per - 1); return state + ((tl >> "
+  // rev != 0 walks an instance's tiles in descending order (tile index bits
+  // complemented), so a pass that follows an ascending one starts on the
+  // amplitudes written last, which are still in L2
+  o << "  const u64 rmask = rev ? (u64)(tiles_per - 1) : 0ull;\n";
+  o << "  auto gaddr = [&](long long tl) { const u64 ti = ((u64)tl & (u64)(tiles_per - 1)) ^ rmask; return state + ((tl >> "
     << (nb - t) << ") << " << nb << ") + " << pdep_expr("ti", outer) << "; };\n";
   o << "  __syncthreads();\n";
   o << kPdlWait;  // the state is read (and written) only after the previous pass completed
@@ -1736,7 +1751,8 @@ int jit_launch(const JitModule& m, const Schedule& s, int p, int n_bits, int sm_
   const unsigned grid = static_cast<unsigned>(std::max<int64_t>(1, std::min(ntiles, cap)));
   long long bs = bstride;
   const int32_t* mc = static_cast<const int32_t*>(m.mc) + m.mc_off[p];
-  void* args[] = {&state, &batch, const_cast<void**>(&bmat), &bs, &mc, &out};
+  int rev = alternate_tile_order() ? (p & 1) : 0;
+  void* args[] = {&state, &batch, const_cast<void**>(&bmat), &bs, &mc, &out, &rev};
   if (launch_pass(f, grid, static_cast<unsigned>(threads), static_cast<unsigned>(smem), st, args, kPdlFwd) !=
       CUDA_SUCCESS) {
     set_error("cuLaunchKernel failed for a specialised pass");
