@@ -816,7 +816,8 @@ void emit_adj_pass(std::ostringstream& o, const jq_plan* plan, const Schedule& s
   const int nthr = 1 << (t - rb);
   const int nr = 1 << rb;
   // both tiles' register blocks are live: allow up to 255 registers a thread
-  const int minb = std::max(1, std::min(8, 65536 / (nthr * 256)));
+  int minb = std::max(1, std::min(8, 65536 / (nthr * 256)));
+  if (const char* e = std::getenv("JQ_JIT_AMINB")) minb = std::max(1, std::min(16, std::atoi(e)));
   const uint64_t full = (nb >= 64) ? ~0ULL : ((1ULL << nb) - 1);
   const uint64_t outer = full & ~pd.tile_mask;
   const int smat_pad = (pd.smat_len + 1) & ~1;
