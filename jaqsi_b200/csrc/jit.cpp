@@ -454,6 +454,17 @@ int jit_bufs() {
   return n;
 }
 
+// One-qubit dense blocks of forward passes read their matrix as two 16-byte
+// (re, im) loads instead of four broadcast-pair loads (JQ_JIT_COMPACT=0: the
+// broadcast pairs).
+bool compact_mats() {
+  static const bool on = [] {
+    const char* e = std::getenv("JQ_JIT_COMPACT");
+    return !(e && std::atoi(e) == 0);
+  }();
+  return on;
+}
+
 // Tile order of consecutive forward passes: alternately ascending and
 // descending, so that each pass starts on the tiles the pass before it wrote
 // last (24-qubit sweep: -1% a step); JQ_JIT_REV=0 keeps every pass ascending.
@@ -701,10 +712,21 @@ void emit_pass(std::ostringstream& o, const jq_plan* plan, const Schedule& s, in
       else o << "      {\n";
       auto V = [&](int j) { return std::string("v") + std::to_string(var[j]); };
       if (kind == RK_DENSE1 && packed) {
-        o << "        const float4* mq = (const float4*)smatb + " << M << ";\n";
-        o << "        const float4 A = mq[0], Bq = mq[1], Cq = mq[2], Dq = mq[3];\n";
-        o << "        const float2 ar = lo2(A), ai = hi2(A), br = lo2(Bq), bi = hi2(Bq), cr = lo2(Cq), ci = hi2(Cq), "
-             "dr = lo2(Dq), di = hi2(Dq);\n";
+        if (compact_mats() && M % 2 == 0) {
+          // two 16-byte loads of the four (re, im) entries; the broadcast
+          // pairs are formed in registers (half the shared-memory wavefronts
+          // of four broadcast-pair loads)
+          o << "        const float4 m01 = *(const float4*)(smat + " << M << "), m23 = *(const float4*)(smat + "
+            << M + 2 << ");\n";
+          o << "        const float2 ar = make_float2(m01.x, m01.x), ai = make_float2(m01.y, m01.y), "
+               "br = make_float2(m01.z, m01.z), bi = make_float2(m01.w, m01.w), cr = make_float2(m23.x, m23.x), "
+               "ci = make_float2(m23.y, m23.y), dr = make_float2(m23.z, m23.z), di = make_float2(m23.w, m23.w);\n";
+        } else {
+          o << "        const float4* mq = (const float4*)smatb + " << M << ";\n";
+          o << "        const float4 A = mq[0], Bq = mq[1], Cq = mq[2], Dq = mq[3];\n";
+          o << "        const float2 ar = lo2(A), ai = hi2(A), br = lo2(Bq), bi = hi2(Bq), cr = lo2(Cq), ci = hi2(Cq), "
+               "dr = lo2(Dq), di = hi2(Dq);\n";
+        }
         for (int j = 0; j < nr; ++j) {
           if ((j >> q1) & 1) continue;
           if ((static_cast<uint32_t>(j) & crm) != crm) continue;
