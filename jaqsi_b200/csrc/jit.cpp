@@ -465,6 +465,29 @@ bool compact_mats() {
   return on;
 }
 
+// Broadcast pairs (re, re), (im, im) of a complex64 one-qubit matrix at
+// smat[M..M+3] (m00, m01, m10, m11) as ar..di: a b / c d are the rows of G,
+// or of G^dagger (a = conj-free m00, b = m10, c = m01, d = m11; the
+// conjugation is in cdot2c).
+std::string dense1_coefs(uint32_t M, bool dagger, const std::string& ind) {
+  if (compact_mats() && M % 2 == 0) {
+    const char* b = dagger ? "m23.x" : "m01.z";
+    const char* bi = dagger ? "m23.y" : "m01.w";
+    const char* c = dagger ? "m01.z" : "m23.x";
+    const char* ci = dagger ? "m01.w" : "m23.y";
+    return ind + "const float4 m01 = *(const float4*)(smat + " + std::to_string(M) + "), m23 = *(const float4*)(smat + " +
+           std::to_string(M + 2) + ");\n" + ind +
+           "const float2 ar = make_float2(m01.x, m01.x), ai = make_float2(m01.y, m01.y), br = make_float2(" + b + ", " +
+           b + "), bi = make_float2(" + bi + ", " + bi + "), cr = make_float2(" + c + ", " + c + "), ci = make_float2(" +
+           ci + ", " + ci + "), dr = make_float2(m23.z, m23.z), di = make_float2(m23.w, m23.w);\n";
+  }
+  return ind + "const float4* mq = (const float4*)smatb + " + std::to_string(M) + ";\n" + ind +
+         (dagger ? "const float4 A = mq[0], Bq = mq[2], Cq = mq[1], Dq = mq[3];\n"
+                 : "const float4 A = mq[0], Bq = mq[1], Cq = mq[2], Dq = mq[3];\n") +
+         ind + "const float2 ar = lo2(A), ai = hi2(A), br = lo2(Bq), bi = hi2(Bq), cr = lo2(Cq), ci = hi2(Cq), "
+               "dr = lo2(Dq), di = hi2(Dq);\n";
+}
+
 // Tile order of consecutive forward passes: alternately ascending and
 // descending, so that each pass starts on the tiles the pass before it wrote
 // last (24-qubit sweep: -1% a step); JQ_JIT_REV=0 keeps every pass ascending.
@@ -985,10 +1008,7 @@ void emit_adj_pass(std::ostringstream& o, const jq_plan* plan, const Schedule& s
       if (kind == RK_DENSE1) {
         // G^dagger = [[conj m00, conj m10], [conj m01, conj m11]]
         if (c64)
-          o << "          const float4* mq = (const float4*)smatb + " << M << ";\n"
-            << "          const float4 A = mq[0], Bq = mq[2], Cq = mq[1], Dq = mq[3];\n"
-            << "          const float2 ar = lo2(A), ai = hi2(A), br = lo2(Bq), bi = hi2(Bq), cr = lo2(Cq), ci = hi2(Cq), "
-               "dr = lo2(Dq), di = hi2(Dq);\n";
+          o << dense1_coefs(M, true, "          ");
         else
           o << "          const " << T << " h00 = cconj(smat[" << M << "]), h01 = cconj(smat[" << M + 2
             << "]), h10 = cconj(smat[" << M + 1 << "]), h11 = cconj(smat[" << M + 3 << "]);\n";
@@ -1149,10 +1169,7 @@ void emit_fwd_rop(std::ostringstream& o, const RegOp& ro, bool c64, const std::s
   else o << "      {\n";
   if (kind == RK_DENSE1) {
     if (c64) {
-      o << "        const float4* mq = (const float4*)smatb + " << M << ";\n";
-      o << "        const float4 A = mq[0], Bq = mq[1], Cq = mq[2], Dq = mq[3];\n";
-      o << "        const float2 ar = lo2(A), ai = hi2(A), br = lo2(Bq), bi = hi2(Bq), cr = lo2(Cq), ci = hi2(Cq), "
-           "dr = lo2(Dq), di = hi2(Dq);\n";
+      o << dense1_coefs(M, false, "        ");
     } else {
       o << "        const double2 m00 = smat[" << M << "], m01 = smat[" << M + 1 << "], m10 = smat[" << M + 2
         << "], m11 = smat[" << M + 3 << "];\n";
@@ -1437,10 +1454,7 @@ void emit_bwd_pass(std::ostringstream& o, const jq_plan* plan, const Schedule& s
       else o << "        {\n";
       if (kind == RK_DENSE1) {
         if (c64)
-          o << "          const float4* mq = (const float4*)smatb + " << M << ";\n"
-            << "          const float4 A = mq[0], Bq = mq[2], Cq = mq[1], Dq = mq[3];\n"
-            << "          const float2 ar = lo2(A), ai = hi2(A), br = lo2(Bq), bi = hi2(Bq), cr = lo2(Cq), ci = hi2(Cq), "
-               "dr = lo2(Dq), di = hi2(Dq);\n";
+          o << dense1_coefs(M, true, "          ");
         else
           o << "          const double2 h00 = cconj(smat[" << M << "]), h01 = cconj(smat[" << M + 2
             << "]), h10 = cconj(smat[" << M + 1 << "]), h11 = cconj(smat[" << M + 3 << "]);\n";
