@@ -518,9 +518,10 @@ void emit_pass(std::ostringstream& o, const jq_plan* plan, const Schedule& s, in
   const int t = pd.t, c = pd.c, nb = plan->n_bits;
   const int nthr = 1 << (t - rb);
   const int nr = 1 << rb;
-  // register budget: 16 complex64 amplitudes + a 4x4 matrix fit 128 registers;
-  // complex128 needs about 168
-  int minb = std::max(1, std::min(8, 65536 / (nthr * (c64 ? 128 : 168))));
+  // register budget: 16 complex64 amplitudes fit about 100 registers (5
+  // CTAs of 128 threads an SM: 4.29 -> 4.21 ms for the 24-qubit sweep against
+  // 4 CTAs at 128 registers); complex128 needs about 168
+  int minb = std::max(1, std::min(8, 65536 / (nthr * (c64 ? 100 : 168))));
   if (const char* e = std::getenv("JQ_JIT_MINB")) minb = std::max(1, std::min(16, std::atoi(e)));
   // complex64 dense blocks use packed two-lane FMA unless JQ_JIT_SCALAR=1
   const bool packed = c64 && !(std::getenv("JQ_JIT_SCALAR") && std::atoi(std::getenv("JQ_JIT_SCALAR")) == 1);
