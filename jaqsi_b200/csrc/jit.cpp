@@ -469,7 +469,16 @@ bool compact_mats() {
 // smat[M..M+3] (m00, m01, m10, m11) as ar..di: a b / c d are the rows of G,
 // or of G^dagger (a = conj-free m00, b = m10, c = m01, d = m11; the
 // conjugation is in cdot2c).
-std::string dense1_coefs(uint32_t M, bool dagger, const std::string& ind) {
+std::string dense1_coefs(uint32_t M, bool dagger, const std::string& ind, bool su2) {
+  if (su2 && compact_mats() && M % 2 == 0) {
+    // SU(2): one 16-byte load of (m00, m01); m10 = -conj m01, m11 = conj m00
+    const std::string b = dagger ? "-m01.z" : "m01.z", bi = dagger ? "m01.w" : "m01.w";
+    const std::string c = dagger ? "m01.z" : "-m01.z", ci = dagger ? "m01.w" : "m01.w";
+    return ind + "const float4 m01 = *(const float4*)(smat + " + std::to_string(M) + ");\n" + ind +
+           "const float2 ar = make_float2(m01.x, m01.x), ai = make_float2(m01.y, m01.y), br = make_float2(" + b + ", " +
+           b + "), bi = make_float2(" + bi + ", " + bi + "), cr = make_float2(" + c + ", " + c + "), ci = make_float2(" +
+           ci + ", " + ci + "), dr = make_float2(m01.x, m01.x), di = make_float2(-m01.y, -m01.y);\n";
+  }
   if (compact_mats() && M % 2 == 0) {
     const char* b = dagger ? "m23.x" : "m01.z";
     const char* bi = dagger ? "m23.y" : "m01.w";
@@ -737,14 +746,7 @@ void emit_pass(std::ostringstream& o, const jq_plan* plan, const Schedule& s, in
       auto V = [&](int j) { return std::string("v") + std::to_string(var[j]); };
       if (kind == RK_DENSE1 && packed) {
         if (compact_mats() && M % 2 == 0) {
-          // two 16-byte loads of the four (re, im) entries; the broadcast
-          // pairs are formed in registers (half the shared-memory wavefronts
-          // of four broadcast-pair loads)
-          o << "        const float4 m01 = *(const float4*)(smat + " << M << "), m23 = *(const float4*)(smat + "
-            << M + 2 << ");\n";
-          o << "        const float2 ar = make_float2(m01.x, m01.x), ai = make_float2(m01.y, m01.y), "
-               "br = make_float2(m01.z, m01.z), bi = make_float2(m01.w, m01.w), cr = make_float2(m23.x, m23.x), "
-               "ci = make_float2(m23.y, m23.y), dr = make_float2(m23.z, m23.z), di = make_float2(m23.w, m23.w);\n";
+          o << dense1_coefs(M, false, "        ", ro.pad[0] != 0);
         } else {
           o << "        const float4* mq = (const float4*)smatb + " << M << ";\n";
           o << "        const float4 A = mq[0], Bq = mq[1], Cq = mq[2], Dq = mq[3];\n";
@@ -1009,7 +1011,7 @@ void emit_adj_pass(std::ostringstream& o, const jq_plan* plan, const Schedule& s
       if (kind == RK_DENSE1) {
         // G^dagger = [[conj m00, conj m10], [conj m01, conj m11]]
         if (c64)
-          o << dense1_coefs(M, true, "          ");
+          o << dense1_coefs(M, true, "          ", ro.pad[0] != 0);
         else
           o << "          const " << T << " h00 = cconj(smat[" << M << "]), h01 = cconj(smat[" << M + 2
             << "]), h10 = cconj(smat[" << M + 1 << "]), h11 = cconj(smat[" << M + 3 << "]);\n";
@@ -1170,7 +1172,7 @@ void emit_fwd_rop(std::ostringstream& o, const RegOp& ro, bool c64, const std::s
   else o << "      {\n";
   if (kind == RK_DENSE1) {
     if (c64) {
-      o << dense1_coefs(M, false, "        ");
+      o << dense1_coefs(M, false, "        ", ro.pad[0] != 0);
     } else {
       o << "        const double2 m00 = smat[" << M << "], m01 = smat[" << M + 1 << "], m10 = smat[" << M + 2
         << "], m11 = smat[" << M + 3 << "];\n";
@@ -1455,7 +1457,7 @@ void emit_bwd_pass(std::ostringstream& o, const jq_plan* plan, const Schedule& s
       else o << "        {\n";
       if (kind == RK_DENSE1) {
         if (c64)
-          o << dense1_coefs(M, true, "          ");
+          o << dense1_coefs(M, true, "          ", ro.pad[0] != 0);
         else
           o << "          const double2 h00 = cconj(smat[" << M << "]), h01 = cconj(smat[" << M + 2
             << "]), h10 = cconj(smat[" << M + 1 << "]), h11 = cconj(smat[" << M + 3 << "]);\n";

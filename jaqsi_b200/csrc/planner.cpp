@@ -242,7 +242,7 @@ uint32_t swz_bit(int pos, int dtype) {
 // fit in r register bits; an op that does not fit, or that touches a bit of a
 // deferred op, is deferred to a later stage.  Ops with more targets than the
 // register forms cover run as generic shared-memory steps.
-void build_steps(Schedule& s, const std::vector<int32_t>& perm_pool, int dtype) {
+void build_steps(Schedule& s, const std::vector<int32_t>& perm_pool, int dtype, const std::vector<uint8_t>& su2) {
   // register bits per stage (amplitudes per thread = 2^r); JQ_REG_BITS=3
   // selects 8 amplitudes per thread (more threads, more stages)
   int r = 4;
@@ -357,6 +357,9 @@ void build_steps(Schedule& s, const std::vector<int32_t>& perm_pool, int dtype) 
           q1 = qpos(op.tmask[0]);
           q2 = op.kt == 2 ? qpos(op.tmask[1]) : 0;
           mat_len = (1 << op.kt) * (1 << op.kt);
+          // pad[0]: the inner matrix is in SU(2) (m11 = conj m00, m10 = -conj m01)
+          if (op.kt == 1 && op.block >= 0 && op.block < static_cast<int32_t>(su2.size()) && su2[op.block])
+            ro.pad[0] = 1;
         } else if (op.kind == BK_DIAG) {
           kind = RK_DIAG;
           dk = static_cast<uint32_t>(op.kt);
@@ -785,8 +788,23 @@ int build_plan(const jq_op* ops, int n_ops, const jq_obs* obs, int n_obs, int n_
   plan->fwd = schedule(blocks, plan->blocks, nb, tf, c_seed, no_fuse);
   plan->adj = schedule(blocks, plan->blocks, nb, ta, c_seed, no_fuse);
   plan->bwd = schedule(blocks, plan->blocks, nb, ta, c_seed, true);
-  build_steps(plan->fwd, plan->perm_pool, dtype);
-  build_steps(plan->bwd, plan->perm_pool, dtype);
+  // one-wire blocks fused from rotations only (RX, RY, RZ, Rot and their
+  // conjugates) are SU(2) matrices: their passes read half the matrix
+  std::vector<uint8_t> su2(plan->blocks.size(), 0);
+  for (size_t b = 0; b < plan->blocks.size(); ++b) {
+    const DevBlock& blk = plan->blocks[b];
+    if (blk.kind != BK_DENSE || blk.k != 1 || blk.n_ctrl != 0 || blk.prim_end <= blk.prim_begin) continue;
+    bool ok = true;
+    for (int pi = blk.prim_begin; pi < blk.prim_end && ok; ++pi) {
+      const DevPrim& pr = plan->prims[pi];
+      if (pr.op < 0 || (pr.form != PF_U && pr.form != PF_CONJ) || pr.k != 1) { ok = false; break; }
+      const DevOp& dop = plan->ops[pr.op];
+      ok = dop.k == 1 && (dop.kind == JQ_K_RX || dop.kind == JQ_K_RY || dop.kind == JQ_K_RZ || dop.kind == JQ_K_ROT);
+    }
+    su2[b] = ok ? 1 : 0;
+  }
+  build_steps(plan->fwd, plan->perm_pool, dtype, su2);
+  build_steps(plan->bwd, plan->perm_pool, dtype, su2);
   plan->threads = (tune && tune->threads > 0) ? tune->threads : 512;
   if (plan->threads % 32 || plan->threads < 64 || plan->threads > 1024)
     return fail("jq_plan_build: threads must be a multiple of 32 in 64..1024");
