@@ -608,7 +608,29 @@ void emit_pass(std::ostringstream& o, const jq_plan* plan, const Schedule& s, in
     o << "\n";
   }
   const std::string tpl = "<" + std::to_string(t - rb) + ", " + std::to_string(t) + ", " + std::to_string(c) + ">";
-  const std::string pf = (c64 ? "prefetch8t" : "prefetch16t") + tpl;
+  // Tile loads: amplitude l = tid | hi (hi = i << LT) goes to shared offset
+  // swz(tid) ^ swz(hi) from global offset gdep(tid) ^ gdep(hi), both
+  // XOR-linear, so every copy is a per-thread base XOR a literal (no table
+  // lookups; JQ_JIT_PFTBL=1 keeps the table-driven copy)
+  const bool pf_table = std::getenv("JQ_JIT_PFTBL") && std::atoi(std::getenv("JQ_JIT_PFTBL")) == 1;
+  std::string pf = (c64 ? "prefetch8t" : "prefetch16t") + tpl;
+  const char* PFEND = pf_table ? ", tbl)" : ")";
+  if (!pf_table) {
+    const int lt = t - rb;
+    o << "  // tile copy: " << t << " tile bits, the lowest " << c << " contiguous\n";
+    o << "  const u32 pst = " << (c64 ? "swz8" : "swz16") << "(tid);\n";
+    o << "  " << OT << " pgo = 0;";
+    for (int i = 0; i < lt; ++i) o << " if (tid & " << (1u << i) << "u) pgo ^= " << gdep(1ULL << i) << (wide ? "ull;" : "u;");
+    o << "\n";
+    o << "  auto pfx = [&](" << T << "* sd, const " << T << "* gs) {\n";
+    for (int i = 0; i < (1 << (t - lt)); ++i) {
+      const uint64_t hi = static_cast<uint64_t>(i) << lt;
+      o << "    " << (c64 ? "cp_async8" : "cp_async16") << "(sd + (pst ^ " << unswz(hi) << "u), gs + (pgo ^ " << gdep(hi)
+        << (wide ? "ull" : "u") << "));\n";
+    }
+    o << "  };\n";
+    pf = "pfx";
+  }
   o << "  const long long tiles_per = 1ll << " << (nb - t) << ";\n";
   o << "  const long long ntiles = tiles_per * batch;\n";
   // rev != 0 walks an instance's tiles in descending order (tile index bits
@@ -621,7 +643,7 @@ void emit_pass(std::ostringstream& o, const jq_plan* plan, const Schedule& s, in
   o << kPdlWait;  // the state is read (and written) only after the previous pass completed
   for (int j = 0; j + 1 < nbuf; ++j) {
     o << "  if ((long long)blockIdx.x + " << j << "ll * gridDim.x < ntiles) " << pf << "(s0 + " << j * (1 << t)
-      << ", gaddr(blockIdx.x + " << j << "ll * gridDim.x), tbl);\n";
+      << ", gaddr(blockIdx.x + " << j << "ll * gridDim.x)" << PFEND << ";\n";
     o << "  cp_commit();\n";
   }
   o << "  long long last_inst = -1;\n";
@@ -630,7 +652,7 @@ void emit_pass(std::ostringstream& o, const jq_plan* plan, const Schedule& s, in
   o << "    " << T << "* s = s0 + cur * " << (1 << t) << ";\n";
   o << "    { const int nx = cur == 0 ? " << nbuf - 1 << " : cur - 1;  // the buffer computed last\n";
   o << "      const long long ahead = tile + " << nbuf - 1 << "ll * gridDim.x;\n";
-  o << "      if (ahead < ntiles) " << pf << "(s0 + nx * " << (1 << t) << ", gaddr(ahead), tbl); }\n";
+  o << "      if (ahead < ntiles) " << pf << "(s0 + nx * " << (1 << t) << ", gaddr(ahead)" << PFEND << "; }\n";
   o << "    cur = cur + 1 == " << nbuf << " ? 0 : cur + 1;\n";
   o << "    cp_commit();\n";
   o << "    const long long inst = tile >> " << (nb - t) << ";\n";

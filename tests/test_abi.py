@@ -264,7 +264,8 @@ def test_direct_store_addresses_match_tile_layout():
     checked = {"fwd": 0, "adj": 0}
     for k in kernels:
         hb = [int(x) for x in re.search(r"const u32 hb\[\] = \{([^}]*)\}", k).group(1).split(",")]
-        cb = int(re.search(r"prefetch8t<\d+, \d+, (\d+)>", k).group(1))
+        m = re.search(r"prefetch8t<\d+, \d+, (\d+)>", k) or re.search(r"tile copy: \d+ tile bits, the lowest (\d+)", k)
+        cb = int(m.group(1))
 
         def gdep(logical):
             g = 0
