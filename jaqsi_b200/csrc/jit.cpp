@@ -622,6 +622,13 @@ void emit_pass(std::ostringstream& o, const jq_plan* plan, const Schedule& s, in
     o << "  " << OT << " pgo = 0;";
     for (int i = 0; i < lt; ++i) o << " if (tid & " << (1u << i) << "u) pgo ^= " << gdep(1ULL << i) << (wide ? "ull;" : "u;");
     o << "\n";
+    if (c64 && !direct) {  // copy-out base of the pair (2 tid, 2 tid + 1)
+      o << "  const u32 pso0 = swz8(2u * tid), pso1 = swz8(2u * tid + 1u);\n";
+      o << "  " << OT << " pgo2 = 0;";
+      for (int i = 0; i < lt; ++i)
+        o << " if (tid & " << (1u << i) << "u) pgo2 ^= " << gdep(2ULL << i) << (wide ? "ull;" : "u;");
+      o << "\n";
+    }
     o << "  auto pfx = [&](" << T << "* sd, const " << T << "* gs) {\n";
     for (int i = 0; i < (1 << (t - lt)); ++i) {
       const uint64_t hi = static_cast<uint64_t>(i) << lt;
@@ -871,7 +878,28 @@ void emit_pass(std::ostringstream& o, const jq_plan* plan, const Schedule& s, in
   }
   // (direct: the barrier below keeps the next prefetch out of this buffer
   // until every warp has loaded its last stage)
-  if (!direct) o << "    " << (c64 ? "store8t" : "store16t") << tpl << "(s, g, tbl);\n";
+  if (!direct && !pf_table) {
+    // tile copy-out with the same per-thread base / literal split as the
+    // loads (complex64: one 16-byte store of the pair (2 tid | hi, 2 tid | hi | 1))
+    const int lt = t - rb;
+    o << "    {\n";
+    if (c64) {
+      for (int i = 0; i < (1 << (t - 1 - lt)); ++i) {
+        const uint64_t hi = static_cast<uint64_t>(i) << (lt + 1);
+        o << "      { const float2 a = s[pso0 ^ " << unswz(hi) << "u], b = s[pso1 ^ " << unswz(hi)
+          << "u]; __stcs((float4*)(g + (pgo2 ^ " << gdep(hi) << (wide ? "ull" : "u")
+          << ")), make_float4(a.x, a.y, b.x, b.y)); }\n";
+      }
+    } else {
+      for (int i = 0; i < (1 << (t - lt)); ++i) {
+        const uint64_t hi = static_cast<uint64_t>(i) << lt;
+        o << "      __stcs(g + (pgo ^ " << gdep(hi) << (wide ? "ull" : "u") << "), s[pst ^ " << unswz(hi) << "u]);\n";
+      }
+    }
+    o << "    }\n";
+  } else if (!direct) {
+    o << "    " << (c64 ? "store8t" : "store16t") << tpl << "(s, g, tbl);\n";
+  }
   o << "    __syncthreads();\n";
   o << "  }\n}\n";
 }
