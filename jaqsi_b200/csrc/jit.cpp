@@ -454,6 +454,36 @@ int jit_bufs() {
   return n;
 }
 
+// Tile load with literal offsets: amplitude l = tid | (i << lt) goes to
+// shared offset swz(tid) ^ swz(i << lt) from global offset gdep(tid) ^
+// gdep(i << lt) (both maps XOR-linear); `sw` and `gd` are those maps.
+template <typename SW, typename GD>
+std::string tile_load_literal(bool c64, int t, int lt, bool wide, SW sw, GD gd, const std::string& sdst,
+                              const std::string& gsrc) {
+  std::ostringstream o;
+  const char* OT = wide ? "u64" : "u32";
+  const char* L = wide ? "ull" : "u";
+  o << "    { const u32 tst = " << (c64 ? "swz8" : "swz16") << "(tid); " << OT << " tgo = 0;";
+  for (int i = 0; i < lt; ++i) o << " if (tid & " << (1u << i) << "u) tgo ^= " << gd(1ULL << i) << L << ";";
+  o << "\n";
+  for (int i = 0; i < (1 << (t - lt)); ++i) {
+    const uint64_t hi = static_cast<uint64_t>(i) << lt;
+    o << "      " << (c64 ? "cp_async8" : "cp_async16") << "(" << sdst << " + (tst ^ " << sw(hi) << "u), " << gsrc
+      << " + (tgo ^ " << gd(hi) << L << "));\n";
+  }
+  o << "    }\n";
+  return o.str();
+}
+
+// JQ_JIT_PFTBL=1: tile loads through the shared-memory deposit table
+bool pf_table_env() {
+  static const bool on = [] {
+    const char* e = std::getenv("JQ_JIT_PFTBL");
+    return e && std::atoi(e) == 1;
+  }();
+  return on;
+}
+
 // One-qubit dense blocks of forward passes read their matrix as two 16-byte
 // (re, im) loads instead of four broadcast-pair loads (JQ_JIT_COMPACT=0: the
 // broadcast pairs).
@@ -1016,8 +1046,14 @@ void emit_adj_pass(std::ostringstream& o, const jq_plan* plan, const Schedule& s
     o << "        for (int e = tid; e < n; e += blockDim.x) smat[d + e] = bm[a + e]; }\n";
   o << "      (void)bm; last_inst = inst;\n      __syncthreads();\n    }\n";
   const std::string tpl = "<" + std::to_string(t - rb) + ", " + std::to_string(t) + ", " + std::to_string(c) + ">";
-  o << "    " << (c64 ? "prefetch8t" : "prefetch16t") << tpl << "(sp, psi + goff, tbl);\n";
-  o << "    " << (c64 ? "prefetch8t" : "prefetch16t") << tpl << "(sl, lam + goff, tbl);\n";
+  if (pf_table_env()) {
+    o << "    " << (c64 ? "prefetch8t" : "prefetch16t") << tpl << "(sp, psi + goff, tbl);\n";
+    o << "    " << (c64 ? "prefetch8t" : "prefetch16t") << tpl << "(sl, lam + goff, tbl);\n";
+  } else {
+    o << "    // tile copy: " << t << " tile bits, the lowest " << c << " contiguous\n";
+    o << tile_load_literal(c64, t, t - rb, wide, unswz, gdep, "sp", "psi + goff");
+    o << tile_load_literal(c64, t, t - rb, wide, unswz, gdep, "sl", "lam + goff");
+  }
   o << "    cp_commit();\n    cp_wait0();\n";
   o << "    __syncthreads();\n";
   for (int si = pd.step_end - 1; si >= pd.step_begin; --si) {
@@ -1423,8 +1459,14 @@ void emit_bwd_pass(std::ostringstream& o, const jq_plan* plan, const Schedule& s
     o << "        for (int e = tid; e < n; e += blockDim.x) smat[d + e] = bm[a + e]; }\n";
   o << "      (void)bm; last_inst = inst;\n      __syncthreads();\n    }\n";
   const std::string tpl = "<" + std::to_string(t - rb) + ", " + std::to_string(t) + ", " + std::to_string(c) + ">";
-  o << "    " << (c64 ? "prefetch8t" : "prefetch16t") << tpl << "(sx, xin + goff, tbl);\n";
-  o << "    " << (c64 ? "prefetch8t" : "prefetch16t") << tpl << "(sl, lam + goff, tbl);\n";
+  if (pf_table_env()) {
+    o << "    " << (c64 ? "prefetch8t" : "prefetch16t") << tpl << "(sx, xin + goff, tbl);\n";
+    o << "    " << (c64 ? "prefetch8t" : "prefetch16t") << tpl << "(sl, lam + goff, tbl);\n";
+  } else {
+    o << "    // tile copy: " << t << " tile bits, the lowest " << c << " contiguous\n";
+    o << tile_load_literal(c64, t, t - rb, wide, unswz, gdep, "sx", "xin + goff");
+    o << tile_load_literal(c64, t, t - rb, wide, unswz, gdep, "sl", "lam + goff");
+  }
   o << "    cp_commit();\n    cp_wait0();\n";
   o << "    __syncthreads();\n";
   // forward walk: stage k reads tile k and writes tile k + 1
